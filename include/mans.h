@@ -1,0 +1,128 @@
+/*
+ * mans.h -- C ABI of the B200-native MANS codec (libmans_b200.so).
+ *
+ * MANS compresses 16/32-bit integer arrays in two stages: the ADM byte
+ * mapping (a per-group center, one code byte per element and a unary
+ * bit-signal plane, with a prefix-sum compaction), then a warp-interleaved
+ * byte rANS over the mapped bytes. The streams are byte-for-byte those of the
+ * reference implementation (hpdps-group/MANS): the rANS stream is the
+ * coalesced layout of include/ans/GpuANSCodec.h and the uint16 mapping is the
+ * merged layout written by mapping/nv/mappingV15_fused_uint16.cu:933-957.
+ *
+ * All pointers named d_* are device pointers on the calling thread's current
+ * device; all work is enqueued on `stream` and returns without synchronising.
+ * Device buffers passed as inputs or outputs must be 16-byte aligned.
+ * Functions return a mans_status for errors detectable on the host; errors
+ * that depend on the data (an output or workspace that turns out too small, a
+ * corrupt stream, an expired wait) are recorded in the workspace and read
+ * with mans_workspace_status() after the stream has been synchronised.
+ */
+#ifndef MANS_H
+#define MANS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* mans_stream_t; /* binary-compatible with cudaStream_t */
+
+typedef enum mans_status {
+  MANS_OK = 0,
+  MANS_ERR_INVALID_ARG = 1,          /* null pointer, bad dtype, size out of range */
+  MANS_ERR_UNSUPPORTED_PRECISION = 2,/* precision not in {9,10,11} */
+  MANS_ERR_ALIGNMENT = 3,            /* device pointer not 16-byte aligned */
+  MANS_ERR_TOO_LARGE = 4,            /* input exceeds the workspace capacity */
+  MANS_ERR_CUDA = 5,                 /* a CUDA runtime call failed */
+  MANS_ERR_OUT_OF_MEMORY = 6,        /* workspace allocation failed */
+  MANS_ERR_BAD_STREAM = 7,           /* magic, version, precision or sizes invalid */
+  MANS_ERR_OUTPUT_OVERFLOW = 8,      /* compressed stream exceeds out_capacity */
+  MANS_ERR_WORKSPACE_OVERFLOW = 9,   /* mapped bytes exceed the workspace */
+  MANS_ERR_CORRUPT = 10,             /* decode consistency check failed */
+  MANS_ERR_TIMEOUT = 11              /* a bounded device wait expired */
+} mans_status;
+
+typedef enum mans_dtype {
+  MANS_U8 = 1,  /* raw bytes: rANS only (the include/ans codec) */
+  MANS_U16 = 2, /* uint16: ADM unary-signal mapping + rANS */
+  MANS_U32 = 4  /* uint32: ADM escape-byte mapping + rANS */
+} mans_dtype;
+
+typedef struct mans_workspace mans_workspace;
+
+/* ------------------------------------------------------------------------
+ * Workspace: device scratch reused across calls, so a call allocates
+ * nothing. max_input_bytes bounds the uncompressed size of one call;
+ * merged_capacity bounds the mapped (ADM) bytes (0 = 2.1 x max_input_bytes,
+ * which always suffices for MANS_U32 and MANS_U8). A workspace serves one
+ * stream at a time.
+ * ---------------------------------------------------------------------- */
+mans_status mans_workspace_create(mans_workspace** ws, uint64_t max_input_bytes,
+                                  uint64_t merged_capacity);
+mans_status mans_workspace_destroy(mans_workspace* ws);
+/* Device bytes held by the workspace. */
+uint64_t mans_workspace_device_bytes(const mans_workspace* ws);
+/* Synchronise `stream`, then return (and clear) the first device-side error
+ * recorded since the last call; *detail receives e.g. the bytes needed. */
+mans_status mans_workspace_status(mans_workspace* ws, mans_stream_t stream, uint64_t* detail);
+
+/* Upper bound of the compressed size for n elements of dtype when the mapped
+ * bytes fit the default workspace. */
+uint64_t mans_max_compressed_size(mans_dtype dtype, uint64_t n_elems);
+
+/* ------------------------------------------------------------------------
+ * MANS compress: d_out receives the rANS stream of the mapped bytes and
+ * *d_out_size (device, u64) its length. For MANS_U8 this is exactly
+ * multibyte_ans::ansEncode (include/ans/GpuANSEncode.h:286); for MANS_U16 it
+ * is ansEncode applied to the V15 merged buffer of the input.
+ * ---------------------------------------------------------------------- */
+mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in,
+                          uint64_t n_elems, void* d_out, uint64_t out_capacity,
+                          uint64_t* d_out_size, int precision, mans_stream_t stream);
+
+/* MANS decompress of a stream produced by mans_compress. n_elems travels out
+ * of band, as in the reference (examples/compress.cu:79-97). For MANS_U8 this
+ * is multibyte_ans::ansDecode (include/ans/GpuANSDecode.h:379). */
+mans_status mans_decompress(mans_workspace* ws, mans_dtype dtype, const void* d_in,
+                            uint64_t in_size, void* d_out, uint64_t n_elems,
+                            mans_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Reference-compatible rANS entry points (include/ans, src/GpuANS.cu). Same
+ * arguments and meaning as the reference; they run on a library-owned
+ * workspace per (device, stream) that is created on first use, so the first
+ * call on a stream allocates. Errors the reference could only print are
+ * returned as a status.
+ * ---------------------------------------------------------------------- */
+/* multibyte_ans::ansEncode, include/ans/GpuANSEncode.h:286. d_out must hold
+ * mans_ans_max_compressed_size(in_size) bytes; *d_out_size is a device u32. */
+mans_status mans_ans_encode(int precision, const uint8_t* d_in, uint32_t in_size,
+                            uint8_t* d_out, uint32_t* d_out_size, mans_stream_t stream);
+/* multibyte_ans::ansDecode, include/ans/GpuANSDecode.h:379. d_out must hold
+ * the uncompressed size recorded in the stream. */
+mans_status mans_ans_decode(int precision, const uint8_t* d_in, uint8_t* d_out,
+                            mans_stream_t stream);
+/* multibyte_ans::ansEncodeBatch / ansDecodeBatch, src/GpuANS.cu:16,33. */
+mans_status mans_ans_encode_batch(int precision, const uint8_t* d_in, uint32_t in_size,
+                                  uint8_t* d_out, uint32_t* d_out_size, mans_stream_t stream);
+mans_status mans_ans_decode_batch(int precision, const uint8_t* d_in, uint8_t* d_out,
+                                  mans_stream_t stream);
+/* multibyte_ans::getMaxCompressedSize, include/ans/GpuANSCodec.h:237. Unlike
+ * the reference's 1.25x estimate this is a true upper bound. */
+uint32_t mans_ans_max_compressed_size(uint32_t in_size);
+/* First device-side error of the library-owned workspace of `stream`. */
+mans_status mans_ans_last_status(mans_stream_t stream, uint64_t* detail);
+
+/* Library version string. */
+const char* mans_version(void);
+
+/* Diagnostic: the encoder's division-table entry {reciprocal, packed} for a
+ * symbol of probability pdf / 2^p and cumulative frequency cdf. */
+void mans_debug_enc_entry(uint32_t pdf, uint32_t cdf, int p, uint32_t out[2]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MANS_H */

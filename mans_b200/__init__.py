@@ -1,0 +1,235 @@
+"""mans_b200 -- B200-native MANS codec (ADM byte mapping + byte rANS).
+
+The product is ``libmans_b200.so`` (C ABI declared in ``include/mans.h``,
+kernels in ``csrc/``). This module loads it with ctypes and offers a thin
+host layer over device tensors. Names follow the reference interface
+(``ansEncode``/``ansDecode``/``getMaxCompressedSize`` of include/ans) plus the
+MANS entry points that add the ADM mapping for uint16/uint32 arrays.
+
+There is no CPU fallback: if the library is missing or no GPU is present the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmans_b200.so")
+
+# mans_status (include/mans.h)
+STATUS = {
+    0: "MANS_OK",
+    1: "MANS_ERR_INVALID_ARG",
+    2: "MANS_ERR_UNSUPPORTED_PRECISION",
+    3: "MANS_ERR_ALIGNMENT",
+    4: "MANS_ERR_TOO_LARGE",
+    5: "MANS_ERR_CUDA",
+    6: "MANS_ERR_OUT_OF_MEMORY",
+    7: "MANS_ERR_BAD_STREAM",
+    8: "MANS_ERR_OUTPUT_OVERFLOW",
+    9: "MANS_ERR_WORKSPACE_OVERFLOW",
+    10: "MANS_ERR_CORRUPT",
+    11: "MANS_ERR_TIMEOUT",
+}
+MANS_U8, MANS_U16, MANS_U32 = 1, 2, 4
+
+# Every symbol include/mans.h declares, with (restype, argtypes).
+_vp, _u64, _u32, _i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int
+SIGNATURES = {
+    "mans_workspace_create": (_i32, [C.POINTER(_vp), _u64, _u64]),
+    "mans_workspace_destroy": (_i32, [_vp]),
+    "mans_workspace_device_bytes": (_u64, [_vp]),
+    "mans_workspace_status": (_i32, [_vp, _vp, C.POINTER(_u64)]),
+    "mans_max_compressed_size": (_u64, [_i32, _u64]),
+    "mans_compress": (_i32, [_vp, _i32, _vp, _u64, _vp, _u64, _vp, _i32, _vp]),
+    "mans_decompress": (_i32, [_vp, _i32, _vp, _u64, _vp, _u64, _vp]),
+    "mans_ans_encode": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
+    "mans_ans_decode": (_i32, [_i32, _vp, _vp, _vp]),
+    "mans_ans_encode_batch": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
+    "mans_ans_decode_batch": (_i32, [_i32, _vp, _vp, _vp]),
+    "mans_ans_max_compressed_size": (_u32, [_u32]),
+    "mans_ans_last_status": (_i32, [_vp, C.POINTER(_u64)]),
+    "mans_version": (C.c_char_p, []),
+    "mans_debug_enc_entry": (None, [_u32, _u32, _i32, C.POINTER(_u32)]),
+}
+
+_LIB: Optional[C.CDLL] = None
+
+
+class MansError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        super().__init__(f"{what}: {STATUS.get(code, code)}" if what else STATUS.get(code, str(code)))
+
+
+def load(build_if_missing: bool = False) -> C.CDLL:
+    """Load libmans_b200.so (raise if it is absent)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise RuntimeError(f"{LIB_PATH} not built; run `python -m mans_b200.build`")
+        from . import build as _b
+        _b.build()
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _check(code: int, what: str) -> None:
+    if code != 0:
+        raise MansError(code, what)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_handle(stream) -> int:
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return int(stream.cuda_stream)
+
+
+_DTYPE_CODE = {"uint8": MANS_U8, "uint16": MANS_U16, "uint32": MANS_U32}
+
+
+def dtype_code(t) -> int:
+    name = str(t.dtype).replace("torch.", "")
+    if name not in _DTYPE_CODE:
+        raise TypeError(f"unsupported dtype {t.dtype}; use uint8, uint16 or uint32")
+    return _DTYPE_CODE[name]
+
+
+def max_compressed_size(dtype: int, n_elems: int) -> int:
+    return int(load().mans_max_compressed_size(dtype, n_elems))
+
+
+def getMaxCompressedSize(in_size: int) -> int:  # noqa: N802 (reference name)
+    """multibyte_ans::getMaxCompressedSize (include/ans/GpuANSCodec.h:237)."""
+    return int(load().mans_ans_max_compressed_size(in_size))
+
+
+class Workspace:
+    """Device scratch reused across calls (mans_workspace_create)."""
+
+    def __init__(self, max_input_bytes: int, merged_capacity: int = 0):
+        lib = load()
+        h = C.c_void_p()
+        _check(lib.mans_workspace_create(C.byref(h), max_input_bytes, merged_capacity),
+               "mans_workspace_create")
+        self.h = h
+        self.max_input_bytes = max_input_bytes
+
+    @property
+    def device_bytes(self) -> int:
+        return int(load().mans_workspace_device_bytes(self.h))
+
+    def status(self, stream=None) -> tuple[int, int]:
+        d = C.c_uint64(0)
+        st = load().mans_workspace_status(self.h, _stream_handle(stream), C.byref(d))
+        return int(st), int(d.value)
+
+    def check(self, stream=None, what: str = "device") -> None:
+        st, det = self.status(stream)
+        if st != 0:
+            raise MansError(st, f"{what} (detail {det})")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            load().mans_workspace_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def compress_into(ws: Workspace, x, out, out_size, precision: int = 10, stream=None) -> None:
+    """Enqueue MANS compress of device tensor x into out (uint8) and out_size (int64[1])."""
+    n = x.numel()
+    code = dtype_code(x)
+    _check(load().mans_compress(ws.h, code, x.data_ptr() if n else None, n, out.data_ptr(),
+                                out.numel(), out_size.data_ptr(), precision,
+                                _stream_handle(stream)), "mans_compress")
+
+
+def decompress_into(ws: Workspace, stream_bytes, in_size: int, out, stream=None) -> None:
+    """Enqueue MANS decompress of stream_bytes[:in_size] into out (dtype decides the mapping)."""
+    n = out.numel()
+    code = dtype_code(out)
+    _check(load().mans_decompress(ws.h, code, stream_bytes.data_ptr(), in_size,
+                                  out.data_ptr() if n else None, n, _stream_handle(stream)),
+           "mans_decompress")
+
+
+def compress(x, precision: int = 10, ws: Optional[Workspace] = None, stream=None):
+    """Compress device tensor x (uint8/uint16/uint32); returns a uint8 tensor (synchronises)."""
+    torch = _torch()
+    n = x.numel()
+    code = dtype_code(x)
+    own = ws is None
+    if own:
+        ws = Workspace(max(n * x.element_size(), 1))
+    cap = max_compressed_size(code, n)
+    out = torch.empty(cap, dtype=torch.uint8, device=x.device)
+    size = torch.zeros(1, dtype=torch.int64, device=x.device)
+    compress_into(ws, x, out, size, precision, stream)
+    ws.check(stream, "mans_compress")
+    nbytes = int(size.item())
+    res = out[:nbytes].clone()
+    if own:
+        ws.close()
+    return res
+
+
+def decompress(s, n: int, dtype, ws: Optional[Workspace] = None, stream=None):
+    """Decompress a stream (device uint8 tensor) of n elements of dtype (synchronises)."""
+    torch = _torch()
+    out = torch.empty(n, dtype=dtype, device=s.device)
+    own = ws is None
+    if own:
+        ws = Workspace(max(n * out.element_size(), 1))
+    decompress_into(ws, s, s.numel(), out, stream)
+    ws.check(stream, "mans_decompress")
+    if own:
+        ws.close()
+    return out
+
+
+# ---- reference-named rANS entry points (include/ans, src/GpuANS.cu) ----
+def ansEncode(precision: int, d_in, in_size: int, d_out, d_out_size, stream=None) -> None:  # noqa: N802
+    """multibyte_ans::ansEncode (include/ans/GpuANSEncode.h:286); d_out_size is a device uint32/int32[1]."""
+    _check(load().mans_ans_encode(precision, d_in.data_ptr(), in_size, d_out.data_ptr(),
+                                  d_out_size.data_ptr(), _stream_handle(stream)), "ansEncode")
+
+
+def ansDecode(precision: int, d_in, d_out, stream=None) -> None:  # noqa: N802
+    """multibyte_ans::ansDecode (include/ans/GpuANSDecode.h:379)."""
+    _check(load().mans_ans_decode(precision, d_in.data_ptr(), d_out.data_ptr(),
+                                  _stream_handle(stream)), "ansDecode")
+
+
+ansEncodeBatch = ansEncode  # src/GpuANS.cu:16 forwards to ansEncode
+ansDecodeBatch = ansDecode  # src/GpuANS.cu:33 forwards to ansDecode
+
+
+def ans_last_status(stream=None) -> tuple[int, int]:
+    d = C.c_uint64(0)
+    st = load().mans_ans_last_status(_stream_handle(stream), C.byref(d))
+    return int(st), int(d.value)
+
+
+def version() -> str:
+    return load().mans_version().decode()

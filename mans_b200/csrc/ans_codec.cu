@@ -1,0 +1,422 @@
+// ans_codec.cu -- byte rANS over 4 KiB blocks for sm_100a: histogram,
+// encode (with single-pass output compaction) and decode.
+//
+// Stream layout and arithmetic are those of include/ans (GpuANSCodec.h,
+// GpuANSEncode.h, GpuANSDecode.h); the kernels are organised differently:
+//  * encode writes the final coalesced stream directly: each warp stages its
+//    block's words in shared memory, learns its word offset through a
+//    decoupled look-back over per-block flags, and stores 16-byte vectors.
+//    The reference instead writes an uncoalesced scratch (5,248-byte stride),
+//    scans with up to three kernels and copies with a fourth.
+//  * the table is normalised by the last CTA of the histogram kernel, not by
+//    a separate launch;
+//  * decode validates the header on the device and reports a status instead
+//    of device asserts, and checks that every block consumes exactly its
+//    words and returns to the start state.
+#include "ans_table.cuh"
+#include "mans_internal.h"
+#include "smem_io.cuh"
+
+namespace mans {
+
+// ------------------------------------------------------------------------
+// Histogram of a raw byte buffer (GpuANSStatistics.h:24-151), with per-warp
+// shared-memory bins merged into the global histogram once per CTA.
+// ------------------------------------------------------------------------
+constexpr int kHistThreads = 256;
+
+__device__ __forceinline__ void hist_word(uint32_t* h, uint32_t w) {
+  atomicAdd(&h[w & 0xff], 1u);
+  atomicAdd(&h[(w >> 8) & 0xff], 1u);
+  atomicAdd(&h[(w >> 16) & 0xff], 1u);
+  atomicAdd(&h[w >> 24], 1u);
+}
+
+__global__ __launch_bounds__(kHistThreads) void hist_bytes_kernel(const uint8_t* __restrict__ in,
+                                                                  uint64_t n, Ctrl* ctrl,
+                                                                  int prob_bits) {
+  __shared__ uint32_t s_h[kHistThreads / 32][kAnsSyms];
+  const int t = threadIdx.x, warp = t >> 5;
+  for (int i = t; i < (kHistThreads / 32) * kAnsSyms; i += kHistThreads) (&s_h[0][0])[i] = 0;
+  __syncthreads();
+  uint32_t* h = s_h[warp];
+  const uint64_t n16 = n >> 4;
+  const uint4* in4 = reinterpret_cast<const uint4*>(in);
+  for (uint64_t i = (uint64_t)blockIdx.x * kHistThreads + t; i < n16;
+       i += (uint64_t)gridDim.x * kHistThreads) {
+    uint4 v = __ldcs(in4 + i);
+    hist_word(h, v.x);
+    hist_word(h, v.y);
+    hist_word(h, v.z);
+    hist_word(h, v.w);
+  }
+  if (blockIdx.x == 0) {
+    uint64_t i = (n16 << 4) + t;
+    if (i < n) atomicAdd(&h[in[i]], 1u);
+  }
+  hist_merge_and_normalize(s_h, kHistThreads / 32, ctrl, n, 0, prob_bits);
+}
+
+// ------------------------------------------------------------------------
+// Encode (GpuANSEncode.h:25-164 arithmetic, :181-284 layout).
+// ------------------------------------------------------------------------
+constexpr int kEncWarps = 4;
+constexpr int kEncThreads = kEncWarps * 32;
+constexpr uint32_t kEncOutWords = kAnsMaxBlockWords + 8;
+
+struct EncSmem {
+  uint2 table[kAnsSyms];
+  alignas(16) uint8_t in[kEncWarps][kAnsBlock + 16];
+  alignas(16) uint16_t out[kEncWarps][kEncOutWords];
+};
+
+// One interleaved step: renormalise (emit 16 bits, lanes in ascending order
+// into the compacted word buffer), then x = (x/pdf << p) + x%pdf + cdf.
+__device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
+                                         const uint2* __restrict__ tab, uint16_t* __restrict__ out,
+                                         uint32_t& nw, int p, uint32_t ltmask) {
+  const uint2 e = tab[sym];
+  const uint32_t cmpl = (e.y >> 13) & 0xfffu;
+  const uint32_t thr = ((1u << p) - cmpl) << (kAnsStateBits - p);
+  const bool wr = valid && x >= thr;
+  const uint32_t vote = __ballot_sync(0xffffffffu, wr);
+  if (wr) {
+    out[nw + __popc(vote & ltmask)] = (uint16_t)(x & 0xffffu);
+    x >>= 16;
+  }
+  nw += __popc(vote);
+  if (valid) {
+    const uint32_t q = __umulhi(x, e.x) >> (e.y >> 25);
+    x = x + (e.y & 0x1fffu) + q * cmpl;
+  }
+}
+
+__global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
+    const uint8_t* __restrict__ in, uint8_t* __restrict__ out, uint64_t out_cap,
+    unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
+    unsigned long long* flags, uint32_t epoch, int p) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  EncSmem& sm = *reinterpret_cast<EncSmem*>(smem_raw);
+  __shared__ int s_last;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const uint32_t ltmask = lanemask_lt();
+
+  const bool failed = *((volatile uint32_t*)&ctrl->status) != 0;
+  const uint64_t n = __ldcg(&ctrl->merged_size);
+  const uint64_t nb = div_up_u64(n, kAnsBlock);
+  const uint64_t over = ans_overhead(nb);
+
+  if (!failed) {
+    for (int i = t; i < kAnsSyms; i += kEncThreads) sm.table[i] = ctrl->enc_table[i];
+  }
+  __syncthreads();
+
+  if (!failed && nb == 0 && blockIdx.x == 0 && warp == 0) {
+    // Empty input: header and a zero pdf only (GpuANSEncode.h:201-237).
+    if (over > out_cap) {
+      if (lane == 0) report_error(ctrl, MANS_ERR_OUTPUT_OVERFLOW, over);
+    } else {
+      if (lane < 8) {
+        uint32_t hv[8] = {kAnsMagicVersion, 0, 0, 0, (uint32_t)p, 0, 0, 0};
+        reinterpret_cast<uint32_t*>(out)[lane] = hv[lane];
+      }
+      for (int i = lane; i < kAnsSyms; i += 32)
+        reinterpret_cast<uint16_t*>(out + kAnsHeaderBytes)[i] = (uint16_t)ctrl->pdf[i];
+      if (lane == 0) {
+        if (out_size64) *out_size64 = over;
+        if (out_size32) *out_size32 = (uint32_t)over;
+      }
+    }
+  }
+
+  while (!failed) {
+    uint32_t b = 0;
+    if (lane == 0) b = atomicAdd(&ctrl->tile_counter[1], 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if (b >= nb) break;
+    const uint64_t start = (uint64_t)b * kAnsBlock;
+    const uint32_t bs = (uint32_t)((n - start) < kAnsBlock ? (n - start) : kAnsBlock);
+    uint8_t* sin = sm.in[warp];
+    uint16_t* sout = sm.out[warp];
+    warp_load_phase(sin, in + start, bs, lane);
+    __syncwarp();
+    const uint8_t* syms = sin + phase16(in + start);
+
+    uint32_t x = kAnsStartState, nw = 0;
+    const uint32_t full = bs >> 5;
+    uint32_t j = 0;
+    for (; j + 8 <= full; j += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        enc_step(true, x, syms[(j + u) * 32 + lane], sm.table, sout, nw, p, ltmask);
+    }
+    for (; j < full; ++j) enc_step(true, x, syms[j * 32 + lane], sm.table, sout, nw, p, ltmask);
+    if (bs & 31) {
+      const bool valid = (uint32_t)lane < (bs & 31);
+      enc_step(valid, x, valid ? syms[j * 32 + lane] : 0u, sm.table, sout, nw, p, ltmask);
+    }
+
+    // Pad the word count to a 16-byte multiple with zeros (GpuANSEncode.h:275).
+    const uint32_t padded = (nw + 7) & ~7u;
+    if ((uint32_t)lane < padded - nw) sout[nw + lane] = 0;
+
+    // Single-pass prefix over padded word counts.
+    if (lane == 0)
+      st_release_u64(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, padded));
+    uint32_t prefix = 0;
+    if (b > 0) {
+      prefix = lookback_exclusive(flags, b, epoch, ctrl);
+      if (lane == 0) st_release_u64(&flags[b], make_flag(kFlagIncl, epoch, prefix + padded));
+    }
+    __syncwarp();
+
+    const uint64_t end = over + 2ull * ((uint64_t)prefix + padded);
+    const bool last = (uint64_t)b + 1 == nb;
+    if (last && end > out_cap && lane == 0) report_error(ctrl, MANS_ERR_OUTPUT_OVERFLOW, end);
+    if (end <= out_cap) {
+      uint32_t* states = reinterpret_cast<uint32_t*>(out + kAnsHeaderBytes + 2 * kAnsSyms);
+      states[(uint64_t)b * 32 + lane] = x;
+      uint2* bw = reinterpret_cast<uint2*>(out + kAnsHeaderBytes + 2 * kAnsSyms + 128 * nb);
+      if (lane == 0) bw[b] = make_uint2((bs << 16) | nw, prefix);
+      uint4* dst = reinterpret_cast<uint4*>(out + over + 2ull * prefix);
+      const uint4* src = reinterpret_cast<const uint4*>(sout);
+      for (uint32_t i = lane; i < padded / 8; i += 32) dst[i] = src[i];
+      if (last) {
+        if (lane < 8) {
+          uint32_t hv[8] = {kAnsMagicVersion, (uint32_t)nb, (uint32_t)n, prefix + padded,
+                            (uint32_t)p, 0, 0, 0};
+          reinterpret_cast<uint32_t*>(out)[lane] = hv[lane];
+        }
+        for (int i = lane; i < kAnsSyms; i += 32)
+          reinterpret_cast<uint16_t*>(out + kAnsHeaderBytes)[i] = (uint16_t)ctrl->pdf[i];
+        if (lane == 0 && (nb & 1)) bw[nb] = make_uint2(0, 0);
+        if (lane == 0) {
+          if (out_size64) *out_size64 = end;
+          if (out_size32) *out_size32 = (uint32_t)end;
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  __syncthreads();
+  if (t == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctrl->done_counter[1], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && t == 0) {
+    ctrl->tile_counter[1] = 0;
+    ctrl->done_counter[1] = 0;
+  }
+}
+
+// ------------------------------------------------------------------------
+// Decode (GpuANSDecode.h:27-302; lookup table :307-377).
+// ------------------------------------------------------------------------
+constexpr int kDecWarps = 4;
+constexpr int kDecThreads = kDecWarps * 32;
+constexpr int kMaxProbBits = 11;
+
+struct DecSmem {
+  uint32_t lut[1 << kMaxProbBits];
+  alignas(16) uint16_t in[kDecWarps][kEncOutWords];
+  alignas(16) uint8_t out[kDecWarps][kAnsBlock + 16];
+};
+
+__global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
+    const uint8_t* __restrict__ in, uint64_t in_size, uint8_t* __restrict__ out, uint64_t out_cap,
+    Ctrl* ctrl, int expect_p, int record) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  DecSmem& sm = *reinterpret_cast<DecSmem*>(smem_raw);
+  __shared__ uint32_t s_scan[kDecWarps];
+  __shared__ int s_ok, s_last;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+
+  // ---- header validation (GpuANSCodec.h:106-113 asserts, GpuANSDecode.h:220-227)
+  uint32_t h[5] = {0, 0, 0, 0, 0};
+  bool ok = in_size >= kAnsHeaderBytes + 2 * kAnsSyms;
+  if (ok) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) h[i] = __ldg(reinterpret_cast<const uint32_t*>(in) + i);
+  }
+  const uint32_t nb = h[1], n = h[2], cw = h[3];
+  const int p = (int)(h[4] & 0xfu);
+  ok = ok && h[0] == kAnsMagicVersion && p >= 9 && p <= kMaxProbBits &&
+       (expect_p < 0 || p == expect_p) && (uint64_t)nb == div_up_u64(n, kAnsBlock) &&
+       ans_overhead(nb) + 2ull * cw <= in_size && (uint64_t)n <= out_cap;
+  const bool failed_before = *((volatile uint32_t*)&ctrl->status) != 0;
+  if (t == 0) s_ok = ok && !failed_before;
+  if (!ok && blockIdx.x == 0 && t == 0 && !failed_before)
+    report_error(ctrl, MANS_ERR_BAD_STREAM, 0);
+  if (record && ok && blockIdx.x == 0 && t == 0) ctrl->merged_size = n;
+  __syncthreads();
+
+  if (s_ok && n > 0) {
+    // ---- build the slot -> (cdf_in_bucket, pdf, symbol) table in shared memory
+    const uint16_t* probs = reinterpret_cast<const uint16_t*>(in + kAnsHeaderBytes);
+    uint32_t pdf0 = 0, pdf1 = 0;
+    // thread t holds symbols 2t and 2t+1 (128 threads x 2 = 256)
+    pdf0 = __ldg(probs + 2 * t);
+    pdf1 = __ldg(probs + 2 * t + 1);
+    uint32_t pair = pdf0 + pdf1, incl = pair;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_scan[warp] = incl;
+    __syncthreads();
+    uint32_t base = 0, total = 0;
+    for (int w = 0; w < kDecWarps; ++w) {
+      if (w < warp) base += s_scan[w];
+      total += s_scan[w];
+    }
+    const uint32_t cdf0 = base + incl - pair, cdf1 = cdf0 + pdf0;
+    if (total != (1u << p)) {
+      if (t == 0) {
+        s_ok = 0;
+        if (blockIdx.x == 0) report_error(ctrl, MANS_ERR_BAD_STREAM, 1);
+      }
+    } else {
+      for (uint32_t j = 0; j < pdf0; ++j) sm.lut[cdf0 + j] = (j << 20) | (pdf0 << 8) | (2u * t);
+      for (uint32_t j = 0; j < pdf1; ++j) sm.lut[cdf1 + j] = (j << 20) | (pdf1 << 8) | (2u * t + 1);
+    }
+  }
+  __syncthreads();
+
+  if (s_ok && n > 0) {
+    const uint64_t over = ans_overhead(nb);
+    const uint32_t* states = reinterpret_cast<const uint32_t*>(in + kAnsHeaderBytes + 2 * kAnsSyms);
+    const uint2* bwords = reinterpret_cast<const uint2*>(in + kAnsHeaderBytes + 2 * kAnsSyms + 128ull * nb);
+    const uint8_t* data = in + over;
+    const uint32_t mask = (1u << p) - 1u;
+    const uint32_t gemask = lanemask_ge();
+    uint16_t* sin = sm.in[warp];
+    uint8_t* sout = sm.out[warp];
+    while (true) {
+      uint32_t b = 0;
+      if (lane == 0) b = atomicAdd(&ctrl->tile_counter[2], 1u);
+      b = __shfl_sync(0xffffffffu, b, 0);
+      if (b >= nb) break;
+      uint32_t x = __ldg(states + (uint64_t)b * 32 + lane);
+      const uint2 bw = __ldg(bwords + b);
+      const uint32_t bs = bw.x >> 16, nw = bw.x & 0xffffu, pre = bw.y;
+      const uint32_t expect = (b + 1 == nb) ? n - b * kAnsBlock : kAnsBlock;
+      const uint32_t padded = (nw + 7) & ~7u;
+      if (bs != expect || (uint64_t)pre + padded > cw || padded > kEncOutWords || (pre & 7)) {
+        if (lane == 0) report_error(ctrl, MANS_ERR_CORRUPT, b);
+        continue;
+      }
+      // stage the block's words (16-byte aligned: over % 16 == 0, pre % 8 == 0)
+      const uint4* src = reinterpret_cast<const uint4*>(data + 2ull * pre);
+      for (uint32_t i = lane; i < padded / 8; i += 32) reinterpret_cast<uint4*>(sin)[i] = __ldg(src + i);
+      __syncwarp();
+      uint8_t* dst = out + (uint64_t)b * kAnsBlock;
+      uint8_t* so = sout + phase16(dst);
+      int ptr = (int)nw;
+      bool bad = false;
+      const uint32_t rem = bs & 31;
+      int j = (int)((bs + 31) >> 5) - 1;
+      if (rem) {
+        const bool valid = (uint32_t)lane < rem;
+        if (valid) {
+          const uint32_t e = sm.lut[x & mask];
+          so[j * 32 + lane] = (uint8_t)e;
+          x = ((e >> 8) & 0xfffu) * (x >> p) + (e >> 20);
+        }
+        const bool rd = valid && x < kAnsStartState;
+        const uint32_t vote = __ballot_sync(0xffffffffu, rd);
+        if (rd) {
+          const int idx = ptr - __popc(vote & gemask);
+          if (idx >= 0) x = (x << 16) | sin[idx]; else bad = true;
+        }
+        ptr -= __popc(vote);
+        --j;
+      }
+#pragma unroll 4
+      for (; j >= 0; --j) {
+        const uint32_t e = sm.lut[x & mask];
+        so[j * 32 + lane] = (uint8_t)e;
+        x = ((e >> 8) & 0xfffu) * (x >> p) + (e >> 20);
+        const bool rd = x < kAnsStartState;
+        const uint32_t vote = __ballot_sync(0xffffffffu, rd);
+        if (rd) {
+          const int idx = ptr - __popc(vote & gemask);
+          if (idx >= 0) x = (x << 16) | sin[idx]; else bad = true;
+        }
+        ptr -= __popc(vote);
+      }
+      bad = bad || ptr != 0 || x != kAnsStartState;
+      if (__any_sync(0xffffffffu, bad) && lane == 0) report_error(ctrl, MANS_ERR_CORRUPT, b);
+      __syncwarp();
+      warp_store_phase(dst, sout, bs, lane);
+      __syncwarp();
+    }
+  }
+
+  __syncthreads();
+  if (t == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctrl->done_counter[2], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && t == 0) {
+    ctrl->tile_counter[2] = 0;
+    ctrl->done_counter[2] = 0;
+  }
+}
+
+// ------------------------------------------------------------------------
+// Host launchers
+// ------------------------------------------------------------------------
+static int occupancy(const void* fn, int threads, size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem) != cudaSuccess) n = 1;
+  return n > 0 ? n : 1;
+}
+
+void init_ans_launch_cfg(LaunchCfg& cfg) {
+  cudaFuncSetAttribute(ans_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(EncSmem));
+  cudaFuncSetAttribute(ans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(DecSmem));
+  cfg.enc_ctas = occupancy((const void*)ans_encode_kernel, kEncThreads, sizeof(EncSmem));
+  cfg.dec_ctas = occupancy((const void*)ans_decode_kernel, kDecThreads, sizeof(DecSmem));
+  cfg.hist_ctas = occupancy((const void*)hist_bytes_kernel, kHistThreads, 0);
+}
+
+cudaError_t launch_hist_bytes(const uint8_t* in, uint64_t n, Ctrl* ctrl, int prob_bits,
+                              const LaunchCfg& cfg, cudaStream_t s) {
+  uint64_t want = div_up_u64(n >> 4, kHistThreads);
+  uint64_t cap = (uint64_t)cfg.sms * cfg.hist_ctas;
+  unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+  hist_bytes_kernel<<<grid, kHistThreads, 0, s>>>(in, n, ctrl, prob_bits);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ans_encode(const uint8_t* in, uint8_t* out, uint64_t out_cap,
+                              unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
+                              unsigned long long* flags, uint32_t epoch, int prob_bits,
+                              uint64_t max_blocks, const LaunchCfg& cfg, cudaStream_t s) {
+  uint64_t want = div_up_u64(max_blocks, kEncWarps);
+  uint64_t cap = (uint64_t)cfg.sms * cfg.enc_ctas;
+  unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+  ans_encode_kernel<<<grid, kEncThreads, sizeof(EncSmem), s>>>(in, out, out_cap, out_size64,
+                                                                out_size32, ctrl, flags, epoch,
+                                                                prob_bits);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ans_decode(const uint8_t* in, uint64_t in_size, uint8_t* out, uint64_t out_cap,
+                              Ctrl* ctrl, int expect_p, int record, uint64_t max_blocks,
+                              const LaunchCfg& cfg, cudaStream_t s) {
+  uint64_t want = div_up_u64(max_blocks, kDecWarps);
+  uint64_t cap = (uint64_t)cfg.sms * cfg.dec_ctas;
+  unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+  ans_decode_kernel<<<grid, kDecThreads, sizeof(DecSmem), s>>>(in, in_size, out, out_cap, ctrl,
+                                                                expect_p, record);
+  return cudaGetLastError();
+}
+
+}  // namespace mans

@@ -1,0 +1,362 @@
+// mans_capi.cu -- the C ABI of libmans_b200.so (declared in include/mans.h):
+// workspaces, argument checks, kernel dispatch and the reference-compatible
+// rANS entry points.
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <utility>
+
+#include "ans_table.cuh"
+#include "mans_device.cuh"
+#include "mans_internal.h"
+
+namespace mans {
+void init_ans_launch_cfg(LaunchCfg& cfg);
+void init_adm_u16_launch_cfg(LaunchCfg& cfg);
+void init_adm_u32_launch_cfg(LaunchCfg& cfg);
+
+void init_launch_cfg(LaunchCfg& cfg, int device) {
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cfg.sms = sms > 0 ? sms : 148;
+  init_ans_launch_cfg(cfg);
+  init_adm_u16_launch_cfg(cfg);
+  init_adm_u32_launch_cfg(cfg);
+}
+}  // namespace mans
+
+using namespace mans;
+
+struct mans_workspace {
+  int device = 0;
+  uint64_t max_input_bytes = 0;
+  uint64_t merged_cap = 0;
+  uint8_t* base = nullptr;
+  uint64_t bytes = 0;
+  Ctrl* ctrl = nullptr;
+  unsigned long long* adm_flags = nullptr;
+  uint64_t adm_flags_n = 0;
+  unsigned long long* ans_flags = nullptr;
+  uint64_t ans_flags_n = 0;
+  uint8_t* merged = nullptr;  // 16-byte aligned region of merged_cap + slack bytes
+  uint32_t epoch = 0;
+  LaunchCfg cfg;
+};
+
+namespace {
+
+constexpr uint64_t kMaxMerged = 0xfffffff0ull;  // rANS header counts are u32
+constexpr uint64_t kSlack = 256;
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+
+uint32_t next_epoch(mans_workspace* ws) {
+  ws->epoch = (ws->epoch + 1) & 0x3fffffffu;
+  if (ws->epoch == 0) ws->epoch = 1;
+  return ws->epoch;
+}
+
+uint64_t elem_bytes(mans_dtype d) {
+  switch (d) {
+    case MANS_U8: return 1;
+    case MANS_U16: return 2;
+    case MANS_U32: return 4;
+  }
+  return 0;
+}
+
+bool valid_precision(int p) { return p >= 9 && p <= 11; }
+
+// Worst-case rANS stream for n bytes: 32 lanes x 90 words per 4 KiB block.
+uint64_t ans_bound(uint64_t n) {
+  const uint64_t nb = div_up_u64(n, kAnsBlock);
+  return ans_overhead(nb) + nb * (uint64_t)kAnsMaxBlockWords * 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mans_version(void) { return "mans_b200 0.1.0 (sm_100a)"; }
+
+mans_status mans_workspace_create(mans_workspace** out, uint64_t max_input_bytes,
+                                  uint64_t merged_capacity) {
+  if (!out) return MANS_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (merged_capacity == 0) merged_capacity = max_input_bytes / 10 * 21 + 4096;
+  if (merged_capacity > kMaxMerged) merged_capacity = kMaxMerged;
+  auto* ws = new (std::nothrow) mans_workspace();
+  if (!ws) return MANS_ERR_OUT_OF_MEMORY;
+  if (cudaGetDevice(&ws->device) != cudaSuccess) {
+    delete ws;
+    return MANS_ERR_CUDA;
+  }
+  ws->max_input_bytes = max_input_bytes;
+  ws->merged_cap = merged_capacity;
+  // tiles of 4096 elements (ADM) and blocks of 4096 bytes (rANS)
+  ws->adm_flags_n = max_input_bytes / 8192 + 2;
+  uint64_t ans_src = merged_capacity > max_input_bytes ? merged_capacity : max_input_bytes;
+  ws->ans_flags_n = div_up_u64(ans_src, kAnsBlock) + 2;
+  const uint64_t off_ctrl = 0;
+  const uint64_t off_adm = align_up(sizeof(Ctrl), 256);
+  const uint64_t off_ans = align_up(off_adm + 8 * ws->adm_flags_n, 256);
+  const uint64_t off_m = align_up(off_ans + 8 * ws->ans_flags_n, 256);
+  ws->bytes = align_up(off_m + merged_capacity + kSlack, 256);
+  if (cudaMalloc(&ws->base, ws->bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete ws;
+    return MANS_ERR_OUT_OF_MEMORY;
+  }
+  if (cudaMemset(ws->base, 0, off_m) != cudaSuccess) {
+    cudaFree(ws->base);
+    delete ws;
+    return MANS_ERR_CUDA;
+  }
+  ws->ctrl = reinterpret_cast<Ctrl*>(ws->base + off_ctrl);
+  ws->adm_flags = reinterpret_cast<unsigned long long*>(ws->base + off_adm);
+  ws->ans_flags = reinterpret_cast<unsigned long long*>(ws->base + off_ans);
+  ws->merged = ws->base + off_m;
+  init_launch_cfg(ws->cfg, ws->device);
+  *out = ws;
+  return MANS_OK;
+}
+
+mans_status mans_workspace_destroy(mans_workspace* ws) {
+  if (!ws) return MANS_ERR_INVALID_ARG;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ws->device);
+  cudaError_t e = cudaFree(ws->base);
+  cudaSetDevice(prev);
+  delete ws;
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+uint64_t mans_workspace_device_bytes(const mans_workspace* ws) { return ws ? ws->bytes : 0; }
+
+mans_status mans_workspace_status(mans_workspace* ws, mans_stream_t stream, uint64_t* detail) {
+  if (!ws) return MANS_ERR_INVALID_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return MANS_ERR_CUDA;
+  struct {
+    uint32_t status, pad;
+    unsigned long long detail;
+  } h = {0, 0, 0};
+  if (cudaMemcpy(&h, ws->ctrl, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  if (detail) *detail = h.detail;
+  if (h.status != 0) {
+    decltype(h) z = {0, 0, 0};
+    if (cudaMemcpy(ws->ctrl, &z, sizeof(z), cudaMemcpyHostToDevice) != cudaSuccess)
+      return MANS_ERR_CUDA;
+  }
+  return (mans_status)h.status;
+}
+
+uint64_t mans_max_compressed_size(mans_dtype dtype, uint64_t n_elems) {
+  const uint64_t eb = elem_bytes(dtype);
+  if (eb == 0) return 0;
+  const uint64_t in_bytes = n_elems * eb;
+  if (dtype == MANS_U8) return ans_bound(in_bytes);
+  const uint64_t merged = in_bytes / 10 * 21 + 4096;
+  return ans_bound(merged < kMaxMerged ? merged : kMaxMerged);
+}
+
+mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in,
+                          uint64_t n_elems, void* d_out, uint64_t out_capacity,
+                          uint64_t* d_out_size, int precision, mans_stream_t stream) {
+  if (!ws || !d_out || !d_out_size || (!d_in && n_elems)) return MANS_ERR_INVALID_ARG;
+  const uint64_t eb = elem_bytes(dtype);
+  if (eb == 0) return MANS_ERR_INVALID_ARG;
+  if (!valid_precision(precision)) return MANS_ERR_UNSUPPORTED_PRECISION;
+  if ((d_in && !aligned16(d_in)) || !aligned16(d_out)) return MANS_ERR_ALIGNMENT;
+  const uint64_t in_bytes = n_elems * eb;
+  if (in_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  unsigned long long* osz = reinterpret_cast<unsigned long long*>(d_out_size);
+  const uint32_t epoch = next_epoch(ws);
+  cudaError_t e = cudaSuccess;
+  if (dtype == MANS_U8) {
+    if (in_bytes > kMaxMerged) return MANS_ERR_TOO_LARGE;
+    e = launch_hist_bytes((const uint8_t*)d_in, in_bytes, ws->ctrl, precision, ws->cfg, s);
+    if (e == cudaSuccess)
+      e = launch_ans_encode((const uint8_t*)d_in, (uint8_t*)d_out, out_capacity, osz, nullptr,
+                            ws->ctrl, ws->ans_flags, epoch, precision,
+                            div_up_u64(in_bytes, kAnsBlock), ws->cfg, s);
+  } else if (dtype == MANS_U16) {
+    const uint64_t hdr = adm_u16_header_bytes(n_elems);
+    const uint64_t g = div_up_u64(n_elems, kAdmGroup);
+    if (hdr + n_elems + 32 * g > ws->merged_cap) return MANS_ERR_TOO_LARGE;
+    uint8_t* m = ws->merged + merged_pad(hdr);
+    e = launch_adm_u16_map((const uint16_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
+                           ws->adm_flags, epoch, precision, ws->cfg, s);
+    if (e == cudaSuccess)
+      e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
+                            ws->ans_flags, epoch, precision,
+                            div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+  } else {
+    const uint64_t hdr = adm_u32_header_bytes(n_elems);
+    if (hdr + n_elems > ws->merged_cap) return MANS_ERR_TOO_LARGE;
+    uint8_t* m = ws->merged + merged_pad(hdr);
+    e = launch_adm_u32_map((const uint32_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
+                           ws->adm_flags, epoch, precision, ws->cfg, s);
+    if (e == cudaSuccess)
+      e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
+                            ws->ans_flags, epoch, precision,
+                            div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+  }
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+mans_status mans_decompress(mans_workspace* ws, mans_dtype dtype, const void* d_in,
+                            uint64_t in_size, void* d_out, uint64_t n_elems,
+                            mans_stream_t stream) {
+  if (!ws || !d_in || (!d_out && n_elems)) return MANS_ERR_INVALID_ARG;
+  const uint64_t eb = elem_bytes(dtype);
+  if (eb == 0) return MANS_ERR_INVALID_ARG;
+  if (!aligned16(d_in) || (d_out && !aligned16(d_out))) return MANS_ERR_ALIGNMENT;
+  const uint64_t out_bytes = n_elems * eb;
+  if (out_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaSuccess;
+  if (dtype == MANS_U8) {
+    e = launch_ans_decode((const uint8_t*)d_in, in_size, (uint8_t*)d_out, out_bytes, ws->ctrl, -1,
+                          0, div_up_u64(out_bytes, kAnsBlock), ws->cfg, s);
+  } else if (dtype == MANS_U16) {
+    const uint64_t hdr = adm_u16_header_bytes(n_elems);
+    uint8_t* m = ws->merged + merged_pad(hdr);
+    e = launch_ans_decode((const uint8_t*)d_in, in_size, m, ws->merged_cap, ws->ctrl, -1, 1,
+                          div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+    if (e == cudaSuccess)
+      e = launch_adm_u16_unmap(m, n_elems, (uint16_t*)d_out, ws->ctrl, ws->cfg, s);
+  } else {
+    const uint64_t hdr = adm_u32_header_bytes(n_elems);
+    uint8_t* m = ws->merged + merged_pad(hdr);
+    e = launch_ans_decode((const uint8_t*)d_in, in_size, m, ws->merged_cap, ws->ctrl, -1, 1,
+                          div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+    if (e == cudaSuccess)
+      e = launch_adm_u32_unmap(m, n_elems, (uint32_t*)d_out, ws->ctrl, ws->cfg, s);
+  }
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------
+// Reference-compatible entry points on a library-owned workspace per
+// (device, stream). The reference allocates scratch on every call and never
+// frees it (GpuANSEncode.h:298-327, GpuANSDecode.h:386-387); here a call
+// allocates only when the workspace has to grow.
+// ------------------------------------------------------------------------
+namespace {
+std::mutex g_mu;
+std::map<std::pair<int, cudaStream_t>, mans_workspace*> g_ws;
+
+mans_workspace* default_ws(cudaStream_t s, uint64_t need_bytes, mans_status* st) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    *st = MANS_ERR_CUDA;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_mu);
+  auto key = std::make_pair(dev, s);
+  auto it = g_ws.find(key);
+  if (it != g_ws.end() && it->second->max_input_bytes >= need_bytes) {
+    *st = MANS_OK;
+    return it->second;
+  }
+  uint64_t cap = 1ull << 20;
+  if (it != g_ws.end()) {
+    cap = it->second->max_input_bytes * 2;
+    cudaStreamSynchronize(s);
+    mans_workspace_destroy(it->second);
+    g_ws.erase(it);
+  }
+  while (cap < need_bytes) cap *= 2;
+  mans_workspace* ws = nullptr;
+  *st = mans_workspace_create(&ws, cap, 0);
+  if (*st != MANS_OK) return nullptr;
+  g_ws[key] = ws;
+  return ws;
+}
+}  // namespace
+
+extern "C" {
+
+uint32_t mans_ans_max_compressed_size(uint32_t in_size) {
+  const uint64_t b = ans_bound(in_size);
+  return b > 0xffffffffull ? 0xffffffffu : (uint32_t)b;
+}
+
+mans_status mans_ans_encode(int precision, const uint8_t* d_in, uint32_t in_size,
+                            uint8_t* d_out, uint32_t* d_out_size, mans_stream_t stream) {
+  if (!d_out || !d_out_size || (!d_in && in_size)) return MANS_ERR_INVALID_ARG;
+  if (!valid_precision(precision)) return MANS_ERR_UNSUPPORTED_PRECISION;
+  if ((d_in && !aligned16(d_in)) || !aligned16(d_out)) return MANS_ERR_ALIGNMENT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  mans_status st = MANS_OK;
+  mans_workspace* ws = default_ws(s, in_size, &st);
+  if (!ws) return st;
+  const uint32_t epoch = next_epoch(ws);
+  cudaError_t e = launch_hist_bytes(d_in, in_size, ws->ctrl, precision, ws->cfg, s);
+  if (e == cudaSuccess)
+    e = launch_ans_encode(d_in, d_out, ans_bound(in_size), nullptr, d_out_size, ws->ctrl,
+                          ws->ans_flags, epoch, precision, div_up_u64(in_size, kAnsBlock),
+                          ws->cfg, s);
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+mans_status mans_ans_decode(int precision, const uint8_t* d_in, uint8_t* d_out,
+                            mans_stream_t stream) {
+  if (!d_in || !d_out) return MANS_ERR_INVALID_ARG;
+  if (!valid_precision(precision)) return MANS_ERR_UNSUPPORTED_PRECISION;
+  if (!aligned16(d_in) || !aligned16(d_out)) return MANS_ERR_ALIGNMENT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  mans_status st = MANS_OK;
+  mans_workspace* ws = default_ws(s, 0, &st);
+  if (!ws) return st;
+  // Sizes come from the stream header on the device (as in the reference):
+  // the grid is one resident wave and the caller sized d_out from the header.
+  const uint64_t wave = (uint64_t)ws->cfg.sms * ws->cfg.dec_ctas * 4;
+  cudaError_t e = launch_ans_decode(d_in, ~0ull, d_out, ~0ull, ws->ctrl, precision, 0, wave,
+                                    ws->cfg, s);
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+mans_status mans_ans_encode_batch(int precision, const uint8_t* d_in, uint32_t in_size,
+                                  uint8_t* d_out, uint32_t* d_out_size, mans_stream_t stream) {
+  return mans_ans_encode(precision, d_in, in_size, d_out, d_out_size, stream);
+}
+
+mans_status mans_ans_decode_batch(int precision, const uint8_t* d_in, uint8_t* d_out,
+                                  mans_stream_t stream) {
+  return mans_ans_decode(precision, d_in, d_out, stream);
+}
+
+mans_status mans_ans_last_status(mans_stream_t stream, uint64_t* detail) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return MANS_ERR_CUDA;
+  mans_workspace* ws = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto it = g_ws.find(std::make_pair(dev, s));
+    if (it == g_ws.end()) {
+      if (detail) *detail = 0;
+      return MANS_OK;
+    }
+    ws = it->second;
+  }
+  return mans_workspace_status(ws, stream, detail);
+}
+
+// Diagnostic: the encoder's division table entry for (pdf, cdf, p).
+void mans_debug_enc_entry(uint32_t pdf, uint32_t cdf, int p, uint32_t out[2]) {
+  const uint2 e = make_enc_entry(pdf, cdf, p);
+  out[0] = e.x;
+  out[1] = e.y;
+}
+
+}  // extern "C"

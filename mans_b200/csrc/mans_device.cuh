@@ -1,0 +1,146 @@
+// mans_device.cuh -- format constants and device helpers shared by the MANS
+// kernels (sm_100a).
+//
+// Format constants restate include/ans/GpuANSCodec.h:18-61 (rANS stream) and
+// mapping/nv/mappingV15_fused_uint16.cu:16-20 (ADM groups); they are fixed by
+// the stream layout and may not change.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/mans.h"
+
+namespace mans {
+
+// ---- rANS stream (GpuANSCodec.h) ----
+constexpr int kWarp = 32;
+constexpr uint32_t kAnsBlock = 4096;          // kDefaultBlockSize
+constexpr int kAnsSyms = 256;                 // kNumSymbols
+constexpr int kAnsStateBits = 31;             // kANSStateBits
+constexpr uint32_t kAnsStartState = 1u << 15; // kANSStartState == kANSMinState
+constexpr uint32_t kAnsMagicVersion = (0xd00du << 16) | 0x0001u;
+constexpr uint32_t kAnsHeaderBytes = 32;      // sizeof(ANSCoalescedHeader)
+constexpr uint32_t kAnsStepsPerBlock = kAnsBlock / kWarp;  // 128
+// Worst case words of one block: 32 lanes x (128 symbols x 11 bits / 16 + 1).
+constexpr uint32_t kAnsMaxBlockWords = 32 * 90;
+
+__host__ __device__ constexpr uint64_t ans_overhead(uint64_t nb) {
+  return kAnsHeaderBytes + 2 * kAnsSyms + 128 * nb + 8 * ((nb + 1) / 2 * 2);
+}
+
+// ---- ADM groups (mappingV15_fused_uint16.cu, mappingV9_fuse.cu) ----
+constexpr int kAdmChunk = 16;     // elements per lane
+constexpr int kAdmGroup = 512;    // elements per group (one warp)
+constexpr uint32_t kAdmStep = 126;
+constexpr int kAdmGroupsPerTile = 8;  // one CTA of 8 warps maps 8 groups per tile
+
+// ---- device status (first error wins) ----
+struct Ctrl {
+  uint32_t status;        // mans_status of the first device-side error
+  uint32_t pad0;
+  unsigned long long detail;  // e.g. bytes needed
+  uint32_t tile_counter[8];   // dynamic work counters, reset by the last CTA
+  uint32_t done_counter[8];   // CTA completion counters, reset by the last CTA
+  uint32_t hist[kAnsSyms];    // histogram of the merged bytes
+  uint2 enc_table[kAnsSyms];  // {reciprocal, bias | cmpl << 12 | shift << 24}
+  uint32_t pdf[kAnsSyms];
+  unsigned long long merged_size;  // merged bytes of the current call
+  uint32_t total_words;
+  uint32_t pad1;
+};
+
+__device__ __forceinline__ void report_error(Ctrl* c, uint32_t code, unsigned long long detail) {
+  if (atomicCAS(&c->status, 0u, code) == 0u) c->detail = detail;
+}
+
+__device__ __forceinline__ int lane_id() {
+  int l;
+  asm("mov.u32 %0, %%laneid;" : "=r"(l));
+  return l;
+}
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ uint32_t lanemask_ge() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_ge;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// ---- single-pass decoupled look-back (epoch tagged, bounded waits) ----
+// A flag word packs {value:32}{epoch:30}{state:2}; state 1 = aggregate
+// published, 2 = inclusive prefix published. Flags from an older call carry
+// an older epoch and read as "not ready", so the arrays never need clearing.
+constexpr uint32_t kFlagAgg = 1, kFlagIncl = 2;
+__device__ __forceinline__ unsigned long long make_flag(uint32_t state, uint32_t epoch,
+                                                        uint32_t value) {
+  return ((unsigned long long)value << 32) | ((unsigned long long)(epoch & 0x3fffffffu) << 2) |
+         state;
+}
+// Bounded spin: about one second at most (2^20 polls x ~1 us backoff).
+constexpr uint32_t kSpinLimit = 1u << 20;
+
+// Warp-cooperative exclusive prefix of `tile` over flags[0..tile). Every lane
+// returns the same value. On timeout reports MANS_ERR_TIMEOUT and returns the
+// partial sum (the call's output is then invalid, but the kernel finishes).
+__device__ __forceinline__ uint32_t lookback_exclusive(unsigned long long* flags, uint32_t tile,
+                                                       uint32_t epoch, Ctrl* ctrl) {
+  const int lane = lane_id();
+  uint32_t excl = 0;
+  int64_t base = (int64_t)tile - 1;
+  const uint32_t ep = epoch & 0x3fffffffu;
+  while (base >= 0) {
+    int64_t idx = base - lane;
+    unsigned long long w = 0;
+    uint32_t st = kFlagIncl, val = 0;
+    if (idx >= 0) {
+      uint32_t spins = 0, ns = 32;
+      while (true) {
+        w = ld_acquire_u64(&flags[idx]);
+        st = (uint32_t)(w & 3u);
+        uint32_t wep = (uint32_t)((w >> 2) & 0x3fffffffu);
+        if (st != 0 && wep == ep) break;
+        ++spins;
+        // Give up after the bound, or at once when another waiter already
+        // recorded an error (so one expired wait does not multiply).
+        if (spins > kSpinLimit ||
+            ((spins & 63u) == 0 && *((volatile uint32_t*)&ctrl->status) == MANS_ERR_TIMEOUT)) {
+          report_error(ctrl, MANS_ERR_TIMEOUT, tile);
+          st = kFlagIncl;
+          w = 0;
+          break;
+        }
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+      }
+      val = (uint32_t)(w >> 32);
+    }
+    uint32_t incl_mask = __ballot_sync(0xffffffffu, st == kFlagIncl);
+    if (incl_mask) {
+      int first = __ffs(incl_mask) - 1;  // nearest predecessor with a full prefix
+      uint32_t v = lane <= first ? val : 0u;
+      excl += __reduce_add_sync(0xffffffffu, v);
+      break;
+    }
+    excl += __reduce_add_sync(0xffffffffu, val);
+    base -= kWarp;
+  }
+  return excl;
+}
+
+__host__ __device__ inline uint64_t div_up_u64(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline uint64_t min_u64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+}  // namespace mans

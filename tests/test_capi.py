@@ -1,0 +1,82 @@
+"""CPU tests of the C ABI: the library loads, exports every function that
+include/*.h declares, and rejects bad arguments on the host without touching
+a GPU."""
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+import mans_b200 as mb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b(mans_\w+)\s*\(", src, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_library_loads_and_exports_declared_symbols():
+    lib = mb.load()
+    decl = declared_functions()
+    assert len(decl) >= 15
+    for name in decl:
+        assert hasattr(lib, name), name
+        assert name in mb.SIGNATURES, name
+    assert mb.version().startswith("mans_b200")
+
+
+def test_host_side_argument_checks():
+    lib = mb.load()
+    # precision outside {9,10,11}: rejected before any CUDA call
+    assert lib.mans_ans_encode(8, 16, 10, 32, 48, None) == 2
+    assert lib.mans_ans_encode(12, 16, 10, 32, 48, None) == 2
+    assert lib.mans_ans_decode(13, 16, 32, None) == 2
+    # unaligned device pointers
+    assert lib.mans_ans_encode(10, 17, 10, 32, 48, None) == 3
+    assert lib.mans_ans_decode(10, 16, 33, None) == 3
+    # null arguments
+    assert lib.mans_ans_encode(10, 16, 10, None, 48, None) == 1
+    assert lib.mans_compress(None, 2, 16, 10, 32, 100, 48, 10, None) == 1
+    assert lib.mans_decompress(None, 2, 16, 100, 32, 10, None) == 1
+    assert lib.mans_workspace_destroy(None) == 1
+
+
+@pytest.mark.parametrize("n", [0, 1, 4096, 4097, 10 ** 7])
+def test_max_compressed_size_is_a_bound(n, oracle):
+    assert mb.getMaxCompressedSize(n) >= oracle.max_compressed_size(n)
+    assert mb.max_compressed_size(mb.MANS_U8, n) >= oracle.max_compressed_size(n)
+    # uint16: the default workspace admits 2.1x the input bytes of mapped data
+    assert mb.max_compressed_size(mb.MANS_U16, n) >= oracle.max_compressed_size(int(2 * n * 2.1))
+
+
+def test_division_table_is_exact():
+    """x / pdf through the encoder's reciprocal table equals exact division for
+    every pdf and p, on all states the encoder can hold (x < pdf << (31-p))."""
+    lib = mb.load()
+    out = (C.c_uint32 * 2)()
+    rng = np.random.default_rng(0)
+    for p in (9, 10, 11):
+        M = 1 << p
+        for pdf in range(1, M + 1):
+            cdf = int(rng.integers(0, M - pdf + 1))
+            lib.mans_debug_enc_entry(pdf, cdf, p, out)
+            rcp, y = int(out[0]), int(out[1])
+            bias, cmpl, sh = y & 0x1FFF, (y >> 13) & 0xFFF, y >> 25
+            assert cmpl == M - pdf
+            hi = pdf << (31 - p)
+            x = np.concatenate([rng.integers(1, hi, 2000, dtype=np.uint64),
+                                np.array([1, 2, pdf - 1, pdf, pdf + 1, hi - 1], np.uint64)])
+            x = x[(x >= 1) & (x < hi)]
+            q = ((x * np.uint64(rcp)) >> np.uint64(32)) >> np.uint64(sh)
+            got = x + np.uint64(bias) + q * np.uint64(cmpl)
+            want = (x // np.uint64(pdf)) * np.uint64(M) + x % np.uint64(pdf) + np.uint64(cdf)
+            np.testing.assert_array_equal(got, want, err_msg=f"p={p} pdf={pdf}")
