@@ -33,9 +33,18 @@ def _sha(a):
 @pytest.mark.parametrize("case", [c for c in _manifest() if c["kind"] == "adm_u16_cpu"],
                          ids=lambda c: c["name"])
 def test_golden_cpu_mapping(case, oracle):
-    """Oracle uint16 mapping == reference CPU mapping (mappingcpuV2.cpp) output."""
+    """Oracle uint16 mapping == reference CPU mapping (mappingcpuV2.cpp) output.
+
+    Cases outside the reference's defined domain (lanes longer than its
+    32-byte lane buffer, where it fails its own round trip) only require the
+    oracle to round-trip."""
     x = _gen(case["input"], oracle)
     m = oracle.adm_u16_map(x)
+    if not case.get("ref_defined", True):
+        assert not case["ref_roundtrip"]
+        np.testing.assert_array_equal(oracle.adm_u16_unmap(m, x.size), x)
+        return
+    assert case["ref_roundtrip"]
     assert m.size == case["ref_size"]
     assert _sha(m) == case["ref_sha256"]
     if "ref_file" in case:
