@@ -68,6 +68,17 @@ uint64_t mans_workspace_device_bytes(const mans_workspace* ws);
  * recorded since the last call; *detail receives e.g. the bytes needed. */
 mans_status mans_workspace_status(mans_workspace* ws, mans_stream_t stream, uint64_t* detail);
 
+/* Opt-in per-kernel timing: when enabled, CUDA events are recorded on the
+ * call's stream around every kernel of up to 128 compress and 128 decompress
+ * calls (no synchronisation is added). */
+mans_status mans_workspace_set_timing(mans_workspace* ws, int enable);
+/* Summed milliseconds, over the calls recorded since the last read, of the
+ * compress kernels (ms[0] mapping or histogram, ms[1] rANS encode) and the
+ * decompress kernels (ms[2] rANS decode, ms[3] inverse mapping); calls[0..1]
+ * (optional) receive the numbers of compress and decompress calls. Waits for
+ * the recorded events, then clears the record. */
+mans_status mans_workspace_kernel_times(mans_workspace* ws, float ms[4], int calls[2]);
+
 /* Upper bound of the compressed size for n elements of dtype when the mapped
  * bytes fit the default workspace. */
 uint64_t mans_max_compressed_size(mans_dtype dtype, uint64_t n_elems);

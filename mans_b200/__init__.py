@@ -42,6 +42,8 @@ SIGNATURES = {
     "mans_workspace_destroy": (_i32, [_vp]),
     "mans_workspace_device_bytes": (_u64, [_vp]),
     "mans_workspace_status": (_i32, [_vp, _vp, C.POINTER(_u64)]),
+    "mans_workspace_set_timing": (_i32, [_vp, _i32]),
+    "mans_workspace_kernel_times": (_i32, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "mans_max_compressed_size": (_u64, [_i32, _u64]),
     "mans_compress": (_i32, [_vp, _i32, _vp, _u64, _vp, _u64, _vp, _i32, _vp]),
     "mans_decompress": (_i32, [_vp, _i32, _vp, _u64, _vp, _u64, _vp]),
@@ -143,6 +145,17 @@ class Workspace:
         st, det = self.status(stream)
         if st != 0:
             raise MansError(st, f"{what} (detail {det})")
+
+    def set_timing(self, enable: bool = True) -> None:
+        _check(load().mans_workspace_set_timing(self.h, int(enable)), "mans_workspace_set_timing")
+
+    def kernel_times(self) -> dict:
+        """Summed kernel milliseconds and call counts recorded since the last read."""
+        ms = (C.c_float * 4)()
+        calls = (C.c_int * 2)()
+        _check(load().mans_workspace_kernel_times(self.h, ms, calls), "mans_workspace_kernel_times")
+        return {"map": ms[0], "encode": ms[1], "decode": ms[2], "unmap": ms[3],
+                "compress_calls": calls[0], "decompress_calls": calls[1]}
 
     def close(self) -> None:
         if getattr(self, "h", None):

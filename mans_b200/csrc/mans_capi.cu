@@ -42,9 +42,40 @@ struct mans_workspace {
   uint8_t* merged = nullptr;  // 16-byte aligned region of merged_cap + slack bytes
   uint32_t epoch = 0;
   LaunchCfg cfg;
+  // Opt-in kernel timing: a ring of event triples per recorded call
+  // (compress: start, after mapping, after encode; decompress: start, after
+  // decode, after unmapping), read and cleared by mans_workspace_kernel_times.
+  static constexpr int kRing = 128;
+  bool timing = false;
+  cudaEvent_t ev_c[kRing][3] = {};
+  cudaEvent_t ev_d[kRing][3] = {};
+  int nc = 0, nd = 0;  // recorded calls since the last read
 };
 
 namespace {
+
+// i: 0..2 compress marks, 3..5 decompress marks. A call is recorded only
+// while its ring has room (the slot is claimed at the call's first mark).
+inline void mark(mans_workspace* ws, int i, cudaStream_t s) {
+  if (!ws->timing) return;
+  if (i < 3) {
+    if (i == 0) {
+      if (ws->nc >= mans_workspace::kRing) return;
+      ++ws->nc;
+    } else if (ws->nc == 0) {
+      return;
+    }
+    cudaEventRecord(ws->ev_c[ws->nc - 1][i], s);
+  } else {
+    if (i == 3) {
+      if (ws->nd >= mans_workspace::kRing) return;
+      ++ws->nd;
+    } else if (ws->nd == 0) {
+      return;
+    }
+    cudaEventRecord(ws->ev_d[ws->nd - 1][i - 3], s);
+  }
+}
 
 constexpr uint64_t kMaxMerged = 0xfffffff0ull;  // rANS header counts are u32
 constexpr uint64_t kSlack = 256;
@@ -128,6 +159,12 @@ mans_status mans_workspace_destroy(mans_workspace* ws) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(ws->device);
+  for (auto& row : ws->ev_c)
+    for (auto& ev : row)
+      if (ev) cudaEventDestroy(ev);
+  for (auto& row : ws->ev_d)
+    for (auto& ev : row)
+      if (ev) cudaEventDestroy(ev);
   cudaError_t e = cudaFree(ws->base);
   cudaSetDevice(prev);
   delete ws;
@@ -178,9 +215,11 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
   unsigned long long* osz = reinterpret_cast<unsigned long long*>(d_out_size);
   const uint32_t epoch = next_epoch(ws);
   cudaError_t e = cudaSuccess;
+  if (dtype == MANS_U8 && in_bytes > kMaxMerged) return MANS_ERR_TOO_LARGE;
+  mark(ws, 0, s);
   if (dtype == MANS_U8) {
-    if (in_bytes > kMaxMerged) return MANS_ERR_TOO_LARGE;
     e = launch_hist_bytes((const uint8_t*)d_in, in_bytes, ws->ctrl, precision, ws->cfg, s);
+    mark(ws, 1, s);
     if (e == cudaSuccess)
       e = launch_ans_encode((const uint8_t*)d_in, (uint8_t*)d_out, out_capacity, osz, nullptr,
                             ws->ctrl, ws->ans_flags, epoch, precision,
@@ -192,6 +231,7 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
     uint8_t* m = ws->merged + merged_pad(hdr);
     e = launch_adm_u16_map((const uint16_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
                            ws->adm_flags, epoch, precision, ws->cfg, s);
+    mark(ws, 1, s);
     if (e == cudaSuccess)
       e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
                             ws->ans_flags, epoch, precision,
@@ -202,11 +242,13 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
     uint8_t* m = ws->merged + merged_pad(hdr);
     e = launch_adm_u32_map((const uint32_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
                            ws->adm_flags, epoch, precision, ws->cfg, s);
+    mark(ws, 1, s);
     if (e == cudaSuccess)
       e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
                             ws->ans_flags, epoch, precision,
                             div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
   }
+  mark(ws, 2, s);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
 }
 
@@ -221,14 +263,17 @@ mans_status mans_decompress(mans_workspace* ws, mans_dtype dtype, const void* d_
   if (out_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   cudaError_t e = cudaSuccess;
+  mark(ws, 3, s);
   if (dtype == MANS_U8) {
     e = launch_ans_decode((const uint8_t*)d_in, in_size, (uint8_t*)d_out, out_bytes, ws->ctrl, -1,
                           0, div_up_u64(out_bytes, kAnsBlock), ws->cfg, s);
+    mark(ws, 4, s);
   } else if (dtype == MANS_U16) {
     const uint64_t hdr = adm_u16_header_bytes(n_elems);
     uint8_t* m = ws->merged + merged_pad(hdr);
     e = launch_ans_decode((const uint8_t*)d_in, in_size, m, ws->merged_cap, ws->ctrl, -1, 1,
                           div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+    mark(ws, 4, s);
     if (e == cudaSuccess)
       e = launch_adm_u16_unmap(m, n_elems, (uint16_t*)d_out, ws->ctrl, ws->cfg, s);
   } else {
@@ -236,10 +281,56 @@ mans_status mans_decompress(mans_workspace* ws, mans_dtype dtype, const void* d_
     uint8_t* m = ws->merged + merged_pad(hdr);
     e = launch_ans_decode((const uint8_t*)d_in, in_size, m, ws->merged_cap, ws->ctrl, -1, 1,
                           div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+    mark(ws, 4, s);
     if (e == cudaSuccess)
       e = launch_adm_u32_unmap(m, n_elems, (uint32_t*)d_out, ws->ctrl, ws->cfg, s);
   }
+  mark(ws, 5, s);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+mans_status mans_workspace_set_timing(mans_workspace* ws, int enable) {
+  if (!ws) return MANS_ERR_INVALID_ARG;
+  if (enable) {
+    for (auto& row : ws->ev_c)
+      for (auto& ev : row)
+        if (!ev && cudaEventCreate(&ev) != cudaSuccess) return MANS_ERR_CUDA;
+    for (auto& row : ws->ev_d)
+      for (auto& ev : row)
+        if (!ev && cudaEventCreate(&ev) != cudaSuccess) return MANS_ERR_CUDA;
+  }
+  ws->timing = enable != 0;
+  ws->nc = ws->nd = 0;
+  return MANS_OK;
+}
+
+mans_status mans_workspace_kernel_times(mans_workspace* ws, float ms[4], int calls[2]) {
+  if (!ws || !ms) return MANS_ERR_INVALID_ARG;
+  for (int i = 0; i < 4; ++i) ms[i] = 0.f;
+  for (int c = 0; c < ws->nc; ++c) {
+    if (cudaEventSynchronize(ws->ev_c[c][2]) != cudaSuccess) return MANS_ERR_CUDA;
+    float a = 0, b = 0;
+    if (cudaEventElapsedTime(&a, ws->ev_c[c][0], ws->ev_c[c][1]) != cudaSuccess ||
+        cudaEventElapsedTime(&b, ws->ev_c[c][1], ws->ev_c[c][2]) != cudaSuccess)
+      return MANS_ERR_CUDA;
+    ms[0] += a;
+    ms[1] += b;
+  }
+  for (int c = 0; c < ws->nd; ++c) {
+    if (cudaEventSynchronize(ws->ev_d[c][2]) != cudaSuccess) return MANS_ERR_CUDA;
+    float a = 0, b = 0;
+    if (cudaEventElapsedTime(&a, ws->ev_d[c][0], ws->ev_d[c][1]) != cudaSuccess ||
+        cudaEventElapsedTime(&b, ws->ev_d[c][1], ws->ev_d[c][2]) != cudaSuccess)
+      return MANS_ERR_CUDA;
+    ms[2] += a;
+    ms[3] += b;
+  }
+  if (calls) {
+    calls[0] = ws->nc;
+    calls[1] = ws->nd;
+  }
+  ws->nc = ws->nd = 0;
+  return MANS_OK;
 }
 
 }  // extern "C"
