@@ -126,6 +126,19 @@ uint32_t mans_ans_max_compressed_size(uint32_t in_size);
 /* First device-side error of the library-owned workspace of `stream`. */
 mans_status mans_ans_last_status(mans_stream_t stream, uint64_t* detail);
 
+/* rANS encode that allocates nothing, for callers that cannot call
+ * cudaMalloc on their call path (e.g. a real-time loop that cannot absorb
+ * cudaMalloc's latency or implicit synchronisation, or a process whose device
+ * memory is reserved up front by another allocator). No counterpart in the
+ * reference; same arguments and output as mans_ans_encode. Its scratch is a
+ * fixed ~132 KiB device array inside the library, held on every GPU that
+ * loads the library until exit; inputs above 64 MiB are rejected with
+ * MANS_ERR_TOO_LARGE. The first call on a device looks up that array's
+ * address (make it before any stream capture). All calls share the array:
+ * calls that overlap on the GPU race, so issue them on one stream. */
+mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_in, uint32_t in_size,
+                                    uint8_t* d_out, uint32_t* d_out_size, mans_stream_t stream);
+
 /* Library version string. */
 const char* mans_version(void);
 

@@ -53,6 +53,7 @@ SIGNATURES = {
     "mans_ans_decode_batch": (_i32, [_i32, _vp, _vp, _vp]),
     "mans_ans_max_compressed_size": (_u32, [_u32]),
     "mans_ans_last_status": (_i32, [_vp, C.POINTER(_u64)]),
+    "mans_ans_encode_noalloc": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
     "mans_version": (C.c_char_p, []),
     "mans_debug_enc_entry": (None, [_u32, _u32, _i32, C.POINTER(_u32)]),
 }
