@@ -12,12 +12,11 @@
 //   lane in bytes; a shorter lane's final partial byte is filled with 1s.
 // Merged: [i32 exclusive L prefix x g][u16 center x g][u8 code x n][bits].
 //
-// B200 organisation: a CTA of 8 warps maps a tile of 8 groups (4096
-// elements) per iteration, tiles handed out by an atomic counter. The
-// group-length prefix is a single-pass decoupled look-back over tile flags
-// (the reference V15 uses a thrust scan plus a concat kernel above 1,024
-// groups, and an unbounded look-back below), so bits are written once,
-// directly at their final offset. Every byte written is counted in a per-warp
+// B200 organisation: each warp maps one group at a time, groups handed out
+// in order by an atomic counter. The group-length prefix is a single-pass
+// decoupled look-back over per-group flags (the reference V15 uses a thrust
+// scan plus a concat kernel above 1,024 groups, and an unbounded look-back
+// below), so bits are written once, directly at their final offset. Every byte written is counted in a per-warp
 // shared histogram, which gives the rANS histogram of the merged buffer
 // without reading it again; the last CTA normalises the table.
 #include "ans_table.cuh"
@@ -53,18 +52,45 @@ __device__ __forceinline__ uint64_t tail_fill_mask(uint32_t pos) {
   return hi & ~lo;
 }
 
+__device__ __forceinline__ uint32_t claim_group16(uint32_t* counter, int lane) {
+  uint32_t v = 0;
+  if (lane == 0) v = atomicAdd(counter, 1u);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Lane's 16 elements of group grp as 8 packed words (zeros past n).
+__device__ __forceinline__ void load_lane_u16(const uint16_t* __restrict__ in, uint64_t n,
+                                              uint64_t grp, int lane, uint32_t (&w)[8]) {
+  const uint64_t ls = grp * kAdmGroup + (uint64_t)lane * kAdmChunk;
+  if (ls + 16 <= n) {
+    const uint4* src = reinterpret_cast<const uint4*>(in + ls);
+    const uint4 a = __ldcs(src), b = __ldcs(src + 1);
+    w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+    w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint32_t lo = (ls + 2 * i < n) ? in[ls + 2 * i] : 0u;
+      const uint32_t hi = (ls + 2 * i + 1 < n) ? in[ls + 2 * i + 1] : 0u;
+      w[i] = lo | (hi << 16);
+    }
+  }
+}
+
+// One warp maps one group at a time; groups are claimed in order, one at a
+// time (a claim held while another group is mapped would stall every later
+// group's look-back), and the group one grid of warps ahead is prefetched
+// into L2 for whichever warp claims it. The group's bit offset comes from a
+// decoupled look-back over per-group flags.
 __global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
     const uint16_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ M, uint64_t m_cap,
     Ctrl* ctrl, unsigned long long* flags, uint32_t epoch, int prob_bits) {
   __shared__ uint32_t s_h[kMapWarps][kAnsSyms];
-  __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_len[kMapWarps];
-  __shared__ uint32_t s_excl;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   for (int i = t; i < kMapWarps * kAnsSyms; i += kMapThreads) (&s_h[0][0])[i] = 0;
+  __syncthreads();
 
   const uint64_t g = div_up_u64(n, kAdmGroup);
-  const uint64_t ntiles = div_up_u64(g, kMapWarps);
   uint8_t* p_len = M;
   uint8_t* p_ctr = M + 4 * g;
   uint8_t* p_code = M + 6 * g;
@@ -72,41 +98,28 @@ __global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
   const uint64_t bits_base = 6 * g + n;  // offset of the bits section in M
   uint32_t* hist = s_h[warp];
   const bool failed = *((volatile uint32_t*)&ctrl->status) != 0;
-  __syncthreads();
 
+  const uint32_t ahead = gridDim.x * kMapWarps;
   while (!failed) {
-    if (t == 0) s_tile = atomicAdd(&ctrl->tile_counter[0], 1u);
-    __syncthreads();
-    const uint64_t tile = s_tile;
-    if (tile >= ntiles) break;
-    const uint64_t grp = tile * kMapWarps + warp;
-    const bool gvalid = grp < g;
-    const uint64_t gs = grp * kAdmGroup;
-    const uint64_t ls = gs + (uint64_t)lane * kAdmChunk;
-    const int cnt = (!gvalid || ls >= n) ? 0 : (int)min_u64(16, n - ls);
-
-    // ---- load 16 elements (two 16-byte vectors when the lane is full)
-    uint32_t w[8];
-    if (cnt == 16) {
-      const uint4* src = reinterpret_cast<const uint4*>(in + ls);
-      const uint4 a = __ldcs(src), b = __ldcs(src + 1);
-      w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
-      w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
-    } else {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        uint32_t lo = (2 * i < cnt) ? in[ls + 2 * i] : 0u;
-        uint32_t hi = (2 * i + 1 < cnt) ? in[ls + 2 * i + 1] : 0u;
-        w[i] = lo | (hi << 16);
-      }
+    const uint32_t grp = claim_group16(&ctrl->tile_counter[0], lane);
+    if (grp >= g) break;
+    if (lane == 0 && (uint64_t)grp + ahead < g) {
+      const uint64_t ns = ((uint64_t)grp + ahead) * kAdmGroup;
+      prefetch_l2(in + ns, (uint32_t)(2 * min_u64(kAdmGroup, n - ns)));
     }
+    uint32_t w[8];
+    load_lane_u16(in, n, grp, lane, w);
+
+    const uint64_t gs = (uint64_t)grp * kAdmGroup;
+    const uint64_t ls = gs + (uint64_t)lane * kAdmChunk;
+    const int cnt = ls >= n ? 0 : (int)min_u64(16, n - ls);
 
     // ---- center: truncated mean (u32 sum of at most 512 uint16 values)
     uint32_t lsum = 0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) lsum += (w[i] & 0xffffu) + (w[i] >> 16);
     const uint32_t gsum = __reduce_add_sync(0xffffffffu, lsum);
-    const uint32_t gcnt = gvalid ? (uint32_t)min_u64(kAdmGroup, n - gs) : 1u;
+    const uint32_t gcnt = (uint32_t)min_u64(kAdmGroup, n - gs);
     const uint32_t c = gcnt == kAdmGroup ? (gsum >> 9) : gsum / gcnt;
 
     // ---- map: codes, unary bits (first 64 bits in a register), lane length
@@ -125,68 +138,65 @@ __global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
       }
     }
     const uint32_t L = __reduce_max_sync(0xffffffffu, (pos + 7) >> 3);
-    if (lane == 0) s_len[warp] = gvalid ? L : 0u;
-    __syncthreads();
 
-    // ---- tile prefix of group lengths (warp 0: decoupled look-back)
-    if (warp == 0) {
-      const uint32_t my = lane < kMapWarps ? s_len[lane] : 0u;
-      const uint32_t agg = __reduce_add_sync(0xffffffffu, my);
-      if (lane == 0)
-        st_release_u64(&flags[tile], make_flag(tile == 0 ? kFlagIncl : kFlagAgg, epoch, agg));
-      uint32_t excl = 0;
-      if (tile > 0) {
-        excl = lookback_exclusive(flags, (uint32_t)tile, epoch, ctrl);
-        if (lane == 0) st_release_u64(&flags[tile], make_flag(kFlagIncl, epoch, excl + agg));
-      }
-      if (lane == 0) {
-        s_excl = excl;
-        if (tile + 1 == ntiles) {
-          const unsigned long long msize = bits_base + 32ull * (excl + agg);
-          ctrl->merged_size = msize;
-          if (msize > m_cap) report_error(ctrl, MANS_ERR_WORKSPACE_OVERFLOW, msize);
-        }
-      }
-    }
-    __syncthreads();
-    uint32_t gexcl = s_excl;
+    // ---- publish the group length now; the prefix is read after the work
+    //      that does not depend on it
+    if (lane == 0) st_flag(&flags[grp], make_flag(grp == 0 ? kFlagIncl : kFlagAgg, epoch, L));
+
+    // codes: 16-byte aligned (the codes section is aligned by the caller)
+    if (cnt == 16) {
+      *reinterpret_cast<uint4*>(p_code + ls) = make_uint4(codes[0], codes[1], codes[2], codes[3]);
+    } else {
 #pragma unroll
-    for (int i = 0; i < kMapWarps; ++i) gexcl += (i < warp) ? s_len[i] : 0u;
+      for (int i = 0; i < 16; ++i)
+        if (i < cnt) p_code[ls + i] = (uint8_t)(codes[i >> 2] >> ((i & 3) * 8));
+    }
+    // bit bytes of a short lane (< 64 bits): tail fill and histogram now
+    const bool fast = pos < 64;
+    if (fast) {
+      if (pos < 8 * L) acc |= tail_fill_mask(pos);
+      const uint32_t nb8 = L < 8 ? L : 8u;
+      for (uint32_t b = 0; b < nb8; ++b) atomicAdd(&hist[(uint32_t)(acc >> (56 - 8 * b)) & 0xffu], 1u);
+      if (L > 8) atomicAdd(&hist[0], L - 8);
+    }
 
-    if (gvalid) {
-      // lengths (i32, written as two u16: M is only 2-byte aligned here) and center
-      if (lane == 0) {
-        reinterpret_cast<uint16_t*>(p_len + 4 * grp)[0] = (uint16_t)(gexcl & 0xffffu);
-        reinterpret_cast<uint16_t*>(p_len + 4 * grp)[1] = (uint16_t)(gexcl >> 16);
-        reinterpret_cast<uint16_t*>(p_ctr + 2 * grp)[0] = (uint16_t)c;
-        atomicAdd(&hist[gexcl & 0xff], 1u);
-        atomicAdd(&hist[(gexcl >> 8) & 0xff], 1u);
-        atomicAdd(&hist[(gexcl >> 16) & 0xff], 1u);
-        atomicAdd(&hist[gexcl >> 24], 1u);
-        atomicAdd(&hist[c & 0xff], 1u);
-        atomicAdd(&hist[(c >> 8) & 0xff], 1u);
-      }
-      // codes: 16-byte aligned (the codes section is aligned by the caller)
-      if (cnt == 16) {
-        *reinterpret_cast<uint4*>(p_code + ls) = make_uint4(codes[0], codes[1], codes[2], codes[3]);
+    // ---- group bit offset (in units of 32 bytes)
+    uint32_t gexcl = 0;
+    if (grp > 0) {
+      gexcl = lookback_exclusive(flags, grp, epoch, ctrl);
+      if (lane == 0) st_flag(&flags[grp], make_flag(kFlagIncl, epoch, gexcl + L));
+    }
+    if (lane == 0 && (uint64_t)grp + 1 == g) {
+      const unsigned long long msize = bits_base + 32ull * (gexcl + L);
+      ctrl->merged_size = msize;
+      if (msize > m_cap) report_error(ctrl, MANS_ERR_WORKSPACE_OVERFLOW, msize);
+    }
+
+    // lengths (i32, written as two u16: M is only 2-byte aligned here) and center
+    if (lane == 0) {
+      reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[0] = (uint16_t)(gexcl & 0xffffu);
+      reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[1] = (uint16_t)(gexcl >> 16);
+      reinterpret_cast<uint16_t*>(p_ctr + 2ull * grp)[0] = (uint16_t)c;
+      atomicAdd(&hist[gexcl & 0xff], 1u);
+      atomicAdd(&hist[(gexcl >> 8) & 0xff], 1u);
+      atomicAdd(&hist[(gexcl >> 16) & 0xff], 1u);
+      atomicAdd(&hist[gexcl >> 24], 1u);
+      atomicAdd(&hist[c & 0xff], 1u);
+      atomicAdd(&hist[(c >> 8) & 0xff], 1u);
+    }
+    // bits: lane region [32*gexcl + lane*L, +L) of the bits section
+    const uint64_t gend = bits_base + 32ull * ((uint64_t)gexcl + L);
+    if (gend <= m_cap) {
+      uint8_t* dst = p_bits + 32ull * gexcl + (uint64_t)lane * L;
+      if (fast) {
+        for (uint32_t b = 0; b < L; ++b)
+          dst[b] = (uint8_t)(b < 8 ? (uint32_t)(acc >> (56 - 8 * b)) & 0xffu : 0u);
       } else {
-        for (int i = 0; i < cnt; ++i) p_code[ls + i] = (uint8_t)(codes[i >> 2] >> ((i & 3) * 8));
-      }
-      // bits: lane region [32*gexcl + lane*L, +L) of the bits section
-      const uint64_t gend = bits_base + 32ull * ((uint64_t)gexcl + L);
-      if (gend <= m_cap) {
-        uint8_t* dst = p_bits + 32ull * gexcl + (uint64_t)lane * L;
-        if (pos < 64) {
-          if (pos < 8 * L) acc |= tail_fill_mask(pos);
-          for (uint32_t b = 0; b < L; ++b) {
-            const uint32_t byte = b < 8 ? (uint32_t)(acc >> (56 - 8 * b)) & 0xffu : 0u;
-            dst[b] = (uint8_t)byte;
-            atomicAdd(&hist[byte], 1u);
-          }
-        } else {
-          // Long lane: regenerate the stream byte by byte.
-          uint32_t cur = 0, bi = 0, bp = 0;
-          for (int i = 0; i < cnt; ++i) {
+        // Long lane: regenerate the stream byte by byte.
+        uint32_t cur = 0, bi = 0, bp = 0;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          if (i < cnt) {
             uint32_t k, code;
             adm_elem_u16(elem16(w, i), c, k, code);
             while ((bp >> 3) > bi) {
@@ -197,26 +207,25 @@ __global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
             cur |= 0x80u >> (bp & 7);
             bp += k;
           }
-          while ((pos >> 3) > bi) {
-            dst[bi++] = (uint8_t)cur;
-            atomicAdd(&hist[cur], 1u);
-            cur = 0;
-          }
-          if (bi < L) {
-            if (pos < 8 * L) cur |= 0xffu >> (pos & 7);
-            dst[bi++] = (uint8_t)cur;
-            atomicAdd(&hist[cur], 1u);
-          }
-          for (; bi < L; ++bi) {
-            dst[bi] = 0;
-            atomicAdd(&hist[0], 1u);
-          }
+        }
+        while ((pos >> 3) > bi) {
+          dst[bi++] = (uint8_t)cur;
+          atomicAdd(&hist[cur], 1u);
+          cur = 0;
+        }
+        if (bi < L) {
+          if (pos < 8 * L) cur |= 0xffu >> (pos & 7);
+          dst[bi++] = (uint8_t)cur;
+          atomicAdd(&hist[cur], 1u);
+        }
+        for (; bi < L; ++bi) {
+          dst[bi] = 0;
+          atomicAdd(&hist[0], 1u);
         }
       }
     }
-    __syncthreads();
   }
-  hist_merge_and_normalize(s_h, kMapWarps, ctrl, ntiles == 0 ? 0ull : ~0ull, 0, prob_bits);
+  hist_merge_and_normalize(s_h, kMapWarps, ctrl, g == 0 ? 0ull : ~0ull, 0, prob_bits);
 }
 
 // ------------------------------------------------------------------------
@@ -264,7 +273,9 @@ __global__ __launch_bounds__(kUnmapThreads) void adm_u16_unmap_kernel(
       const uint4 v = __ldcs(reinterpret_cast<const uint4*>(p_code + ls));
       codes[0] = v.x; codes[1] = v.y; codes[2] = v.z; codes[3] = v.w;
     } else {
-      for (int i = 0; i < cnt; ++i) codes[i >> 2] |= (uint32_t)p_code[ls + i] << ((i & 3) * 8);
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (i < cnt) codes[i >> 2] |= (uint32_t)p_code[ls + i] << ((i & 3) * 8);
     }
     const uint8_t* src = p_bits + 32ull * ex + (uint64_t)lane * L;
     uint32_t sig[16];
@@ -325,7 +336,9 @@ __global__ __launch_bounds__(kUnmapThreads) void adm_u16_unmap_kernel(
       o[0] = make_uint4(vals[0], vals[1], vals[2], vals[3]);
       o[1] = make_uint4(vals[4], vals[5], vals[6], vals[7]);
     } else {
-      for (int i = 0; i < cnt; ++i) out[ls + i] = (uint16_t)(vals[i >> 1] >> ((i & 1) * 16));
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (i < cnt) out[ls + i] = (uint16_t)(vals[i >> 1] >> ((i & 1) * 16));
     }
   }
 }
@@ -340,9 +353,9 @@ void init_adm_u16_launch_cfg(LaunchCfg& cfg) {
 cudaError_t launch_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* m, uint64_t m_cap,
                                Ctrl* ctrl, unsigned long long* flags, uint32_t epoch,
                                int prob_bits, const LaunchCfg& cfg, cudaStream_t s) {
-  const uint64_t ntiles = div_up_u64(div_up_u64(n, kAdmGroup), kMapWarps);
+  const uint64_t ctas = div_up_u64(div_up_u64(n, kAdmGroup), kMapWarps);
   const uint64_t cap = (uint64_t)cfg.sms * cfg.map_ctas;
-  const unsigned grid = (unsigned)(ntiles < 1 ? 1 : (ntiles < cap ? ntiles : cap));
+  const unsigned grid = (unsigned)(ctas < 1 ? 1 : (ctas < cap ? ctas : cap));
   adm_u16_map_kernel<<<grid, kMapThreads, 0, s>>>(in, n, m, m_cap, ctrl, flags, epoch, prob_bits);
   return cudaGetLastError();
 }

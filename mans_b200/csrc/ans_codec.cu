@@ -59,47 +59,74 @@ __global__ __launch_bounds__(kHistThreads) void hist_bytes_kernel(const uint8_t*
 
 // ------------------------------------------------------------------------
 // Encode (GpuANSEncode.h:25-164 arithmetic, :181-284 layout).
+//
+// One warp encodes one 4 KiB block: lane l codes bytes l, l+32, ... Symbols
+// are read straight from global memory, eight steps ahead of use, from lines
+// prefetched into L1 at the block's start and into L2 one grid of warps
+// earlier. Output words are compacted in a per-warp shared buffer (the
+// only shared staging), then stored as 16-byte vectors once the block's word
+// offset is known.
 // ------------------------------------------------------------------------
-constexpr int kEncWarps = 4;
+constexpr int kEncWarps = 8;
 constexpr int kEncThreads = kEncWarps * 32;
 constexpr uint32_t kEncOutWords = kAnsMaxBlockWords + 8;
+// A block's words compacted in global memory: slots of whole 128-byte lines.
+constexpr uint32_t kEncSlotBytes = (kEncOutWords * 2 + 127) / 128 * 128;
 
 struct EncSmem {
   uint2 table[kAnsSyms];
-  alignas(16) uint8_t in[kEncWarps][kAnsBlock + 16];
   alignas(16) uint16_t out[kEncWarps][kEncOutWords];
+};
+struct EncSmemTableOnly {
+  uint2 table[kAnsSyms];
 };
 
 // One interleaved step: renormalise (emit 16 bits, lanes in ascending order
 // into the compacted word buffer), then x = (x/pdf << p) + x%pdf + cdf.
 __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
                                          const uint2* __restrict__ tab, uint16_t* __restrict__ out,
-                                         uint32_t& nw, int p, uint32_t ltmask) {
+                                         uint32_t& nw, uint32_t mp, uint32_t sh, uint32_t ltmask) {
   const uint2 e = tab[sym];
   const uint32_t cmpl = (e.y >> 13) & 0xfffu;
-  const uint32_t thr = ((1u << p) - cmpl) << (kAnsStateBits - p);
+  const uint32_t thr = (mp - cmpl) << sh;
   const bool wr = valid && x >= thr;
   const uint32_t vote = __ballot_sync(0xffffffffu, wr);
-  if (wr) {
-    out[nw + __popc(vote & ltmask)] = (uint16_t)(x & 0xffffu);
-    x >>= 16;
-  }
+  if (wr) out[nw + __popc(vote & ltmask)] = (uint16_t)(x & 0xffffu);
   nw += __popc(vote);
+  const uint32_t xr = wr ? (x >> 16) : x;
   if (valid) {
-    const uint32_t q = __umulhi(x, e.x) >> (e.y >> 25);
-    x = x + (e.y & 0x1fffu) + q * cmpl;
+    const uint32_t q = __umulhi(xr, e.x) >> (e.y >> 25);
+    x = xr + (e.y & 0x1fffu) + q * cmpl;
+  } else {
+    x = xr;
   }
 }
 
+__device__ __forceinline__ uint32_t claim(uint32_t* counter, int lane) {
+  uint32_t b = 0;
+  if (lane == 0) b = atomicAdd(counter, 1u);
+  return __shfl_sync(0xffffffffu, b, 0);
+}
+
+__device__ __forceinline__ void discard_l2_line(const void* p) {
+  asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
+// kSlots: the block's words are compacted in a per-warp slot of `slots`
+// (global memory, stays in L2 and is discarded after the final copy), so
+// shared memory holds only the coding table. Otherwise they are compacted in
+// shared memory.
+template <bool kSlots>
 __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
     const uint8_t* __restrict__ in, uint8_t* __restrict__ out, uint64_t out_cap,
     unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
-    unsigned long long* flags, uint32_t epoch, int p) {
+    unsigned long long* flags, uint32_t epoch, int p, uint8_t* __restrict__ slots) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  EncSmem& sm = *reinterpret_cast<EncSmem*>(smem_raw);
+  uint2* table = reinterpret_cast<uint2*>(smem_raw);
   __shared__ int s_last;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const uint32_t ltmask = lanemask_lt();
+  const uint32_t mp = 1u << p, sh = kAnsStateBits - p;
 
   const bool failed = *((volatile uint32_t*)&ctrl->status) != 0;
   const uint64_t n = __ldcg(&ctrl->merged_size);
@@ -107,7 +134,7 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
   const uint64_t over = ans_overhead(nb);
 
   if (!failed) {
-    for (int i = t; i < kAnsSyms; i += kEncThreads) sm.table[i] = ctrl->enc_table[i];
+    for (int i = t; i < kAnsSyms; i += kEncThreads) table[i] = ctrl->enc_table[i];
   }
   __syncthreads();
 
@@ -117,8 +144,8 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
       if (lane == 0) report_error(ctrl, MANS_ERR_OUTPUT_OVERFLOW, over);
     } else {
       if (lane < 8) {
-        uint32_t hv[8] = {kAnsMagicVersion, 0, 0, 0, (uint32_t)p, 0, 0, 0};
-        reinterpret_cast<uint32_t*>(out)[lane] = hv[lane];
+        const uint32_t hv = lane == 0 ? kAnsMagicVersion : (lane == 4 ? (uint32_t)p : 0u);
+        reinterpret_cast<uint32_t*>(out)[lane] = hv;
       }
       for (int i = lane; i < kAnsSyms; i += 32)
         reinterpret_cast<uint16_t*>(out + kAnsHeaderBytes)[i] = (uint16_t)ctrl->pdf[i];
@@ -129,31 +156,52 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
     }
   }
 
+  uint16_t* sout;
+  if constexpr (kSlots) {
+    sout = reinterpret_cast<uint16_t*>(slots + ((uint64_t)blockIdx.x * kEncWarps + warp) * kEncSlotBytes);
+  } else {
+    sout = reinterpret_cast<EncSmem*>(smem_raw)->out[warp];
+  }
+  // Blocks are claimed one at a time (a claim held while another block is
+  // encoded would stall every later block's look-back); the block one grid
+  // of warps ahead is prefetched into L2 for whichever warp claims it.
+  const uint32_t ahead = gridDim.x * kEncWarps;
   while (!failed) {
-    uint32_t b = 0;
-    if (lane == 0) b = atomicAdd(&ctrl->tile_counter[1], 1u);
-    b = __shfl_sync(0xffffffffu, b, 0);
+    const uint32_t b = claim(&ctrl->tile_counter[1], lane);
     if (b >= nb) break;
+    if (lane == 0 && (uint64_t)b + ahead < nb) {
+      const uint64_t s1 = ((uint64_t)b + ahead) * kAnsBlock;
+      prefetch_l2(in + s1, (uint32_t)min_u64(kAnsBlock, n - s1));
+    }
     const uint64_t start = (uint64_t)b * kAnsBlock;
-    const uint32_t bs = (uint32_t)((n - start) < kAnsBlock ? (n - start) : kAnsBlock);
-    uint8_t* sin = sm.in[warp];
-    uint16_t* sout = sm.out[warp];
-    warp_load_phase(sin, in + start, bs, lane);
-    __syncwarp();
-    const uint8_t* syms = sin + phase16(in + start);
+    const uint32_t bs = (uint32_t)min_u64(kAnsBlock, n - start);
+    const uint8_t* syms = in + start + lane;
+    if ((uint32_t)lane * 128 < bs) prefetch_l1(in + start + 128 * lane);
 
     uint32_t x = kAnsStartState, nw = 0;
     const uint32_t full = bs >> 5;
     uint32_t j = 0;
-    for (; j + 8 <= full; j += 8) {
+    if (full >= 8) {
+      uint32_t cur[8];
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        enc_step(true, x, syms[(j + u) * 32 + lane], sm.table, sout, nw, p, ltmask);
+      for (int u = 0; u < 8; ++u) cur[u] = __ldg(syms + u * 32);
+      for (; j + 16 <= full; j += 8) {
+        uint32_t nx[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) nx[u] = __ldg(syms + (j + 8 + u) * 32);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) cur[u] = nx[u];
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
+      j += 8;
     }
-    for (; j < full; ++j) enc_step(true, x, syms[j * 32 + lane], sm.table, sout, nw, p, ltmask);
+    for (; j < full; ++j) enc_step(true, x, __ldg(syms + j * 32), table, sout, nw, mp, sh, ltmask);
     if (bs & 31) {
       const bool valid = (uint32_t)lane < (bs & 31);
-      enc_step(valid, x, valid ? syms[j * 32 + lane] : 0u, sm.table, sout, nw, p, ltmask);
+      enc_step(valid, x, valid ? __ldg(syms + j * 32) : 0u, table, sout, nw, mp, sh, ltmask);
     }
 
     // Pad the word count to a 16-byte multiple with zeros (GpuANSEncode.h:275).
@@ -161,12 +209,11 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
     if ((uint32_t)lane < padded - nw) sout[nw + lane] = 0;
 
     // Single-pass prefix over padded word counts.
-    if (lane == 0)
-      st_release_u64(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, padded));
+    if (lane == 0) st_flag(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, padded));
     uint32_t prefix = 0;
     if (b > 0) {
       prefix = lookback_exclusive(flags, b, epoch, ctrl);
-      if (lane == 0) st_release_u64(&flags[b], make_flag(kFlagIncl, epoch, prefix + padded));
+      if (lane == 0) st_flag(&flags[b], make_flag(kFlagIncl, epoch, prefix + padded));
     }
     __syncwarp();
 
@@ -180,12 +227,18 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
       if (lane == 0) bw[b] = make_uint2((bs << 16) | nw, prefix);
       uint4* dst = reinterpret_cast<uint4*>(out + over + 2ull * prefix);
       const uint4* src = reinterpret_cast<const uint4*>(sout);
-      for (uint32_t i = lane; i < padded / 8; i += 32) dst[i] = src[i];
+      for (uint32_t i = lane; i < padded / 8; i += 32) {
+        if constexpr (kSlots) dst[i] = __ldcg(src + i);
+        else dst[i] = src[i];
+      }
       if (last) {
         if (lane < 8) {
-          uint32_t hv[8] = {kAnsMagicVersion, (uint32_t)nb, (uint32_t)n, prefix + padded,
-                            (uint32_t)p, 0, 0, 0};
-          reinterpret_cast<uint32_t*>(out)[lane] = hv[lane];
+          const uint32_t hv = lane == 0 ? kAnsMagicVersion
+                            : lane == 1 ? (uint32_t)nb
+                            : lane == 2 ? (uint32_t)n
+                            : lane == 3 ? prefix + padded
+                            : lane == 4 ? (uint32_t)p : 0u;
+          reinterpret_cast<uint32_t*>(out)[lane] = hv;
         }
         for (int i = lane; i < kAnsSyms; i += 32)
           reinterpret_cast<uint16_t*>(out + kAnsHeaderBytes)[i] = (uint16_t)ctrl->pdf[i];
@@ -197,6 +250,14 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
       }
     }
     __syncwarp();
+    if constexpr (kSlots) {
+      // the slot's lines are consumed: drop them from L2 without write-back
+      const uint32_t lines = (2 * padded + 127) / 128;
+      if ((uint32_t)lane < lines) discard_l2_line(reinterpret_cast<const uint8_t*>(sout) + 128 * lane);
+      if ((uint32_t)lane + 32 < lines)
+        discard_l2_line(reinterpret_cast<const uint8_t*>(sout) + 128 * (lane + 32));
+      __syncwarp();
+    }
   }
 
   __syncthreads();
@@ -213,15 +274,22 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
 
 // ------------------------------------------------------------------------
 // Decode (GpuANSDecode.h:27-302; lookup table :307-377).
+//
+// One warp decodes one block from its last step to its first. The block's
+// words are staged in shared memory (read backwards, data-dependently, every
+// step); decoded bytes go straight to global memory, 32 consecutive bytes per
+// step. The next block is claimed early and its words prefetched into L2.
 // ------------------------------------------------------------------------
-constexpr int kDecWarps = 4;
+constexpr int kDecWarps = 8;
 constexpr int kDecThreads = kDecWarps * 32;
 constexpr int kMaxProbBits = 11;
 
+// Decode table per slot s = state & (2^p - 1): pdf << 16 | (s - cdf) and the
+// symbol (GpuANSDecode.h:27-34 packs the same three fields in one word).
 struct DecSmem {
   uint32_t lut[1 << kMaxProbBits];
+  uint8_t sym[1 << kMaxProbBits];
   alignas(16) uint16_t in[kDecWarps][kEncOutWords];
-  alignas(16) uint8_t out[kDecWarps][kAnsBlock + 16];
 };
 
 __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
@@ -253,16 +321,13 @@ __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
   __syncthreads();
 
   if (s_ok && n > 0) {
-    // ---- build the slot -> (cdf_in_bucket, pdf, symbol) table in shared memory
+    // ---- slot -> (cdf_in_bucket, pdf, symbol) table; thread t owns symbol t
     const uint16_t* probs = reinterpret_cast<const uint16_t*>(in + kAnsHeaderBytes);
-    uint32_t pdf0 = 0, pdf1 = 0;
-    // thread t holds symbols 2t and 2t+1 (128 threads x 2 = 256)
-    pdf0 = __ldg(probs + 2 * t);
-    pdf1 = __ldg(probs + 2 * t + 1);
-    uint32_t pair = pdf0 + pdf1, incl = pair;
+    const uint32_t pdf = __ldg(probs + t);
+    uint32_t incl = pdf;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += v;
     }
     if (lane == 31) s_scan[warp] = incl;
@@ -272,15 +337,17 @@ __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
       if (w < warp) base += s_scan[w];
       total += s_scan[w];
     }
-    const uint32_t cdf0 = base + incl - pair, cdf1 = cdf0 + pdf0;
+    const uint32_t cdf = base + incl - pdf;
     if (total != (1u << p)) {
       if (t == 0) {
         s_ok = 0;
         if (blockIdx.x == 0) report_error(ctrl, MANS_ERR_BAD_STREAM, 1);
       }
     } else {
-      for (uint32_t j = 0; j < pdf0; ++j) sm.lut[cdf0 + j] = (j << 20) | (pdf0 << 8) | (2u * t);
-      for (uint32_t j = 0; j < pdf1; ++j) sm.lut[cdf1 + j] = (j << 20) | (pdf1 << 8) | (2u * t + 1);
+      for (uint32_t j = 0; j < pdf; ++j) {
+        sm.lut[cdf + j] = (pdf << 16) | j;
+        sm.sym[cdf + j] = (uint8_t)t;
+      }
     }
   }
   __syncthreads();
@@ -293,65 +360,64 @@ __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
     const uint32_t mask = (1u << p) - 1u;
     const uint32_t gemask = lanemask_ge();
     uint16_t* sin = sm.in[warp];
-    uint8_t* sout = sm.out[warp];
-    while (true) {
-      uint32_t b = 0;
-      if (lane == 0) b = atomicAdd(&ctrl->tile_counter[2], 1u);
-      b = __shfl_sync(0xffffffffu, b, 0);
-      if (b >= nb) break;
+    uint32_t b = claim(&ctrl->tile_counter[2], lane);
+    while (b < nb) {
+      const uint32_t nxt = claim(&ctrl->tile_counter[2], lane);
       uint32_t x = __ldg(states + (uint64_t)b * 32 + lane);
       const uint2 bw = __ldg(bwords + b);
+      if (nxt < nb && lane == 0) {
+        const uint2 bn = __ldg(bwords + nxt);
+        const uint32_t wn = ((bn.x & 0xffffu) + 7) & ~7u;
+        if ((uint64_t)bn.y + wn <= cw) prefetch_l2(data + 2ull * bn.y, 2 * wn);
+      }
       const uint32_t bs = bw.x >> 16, nw = bw.x & 0xffffu, pre = bw.y;
       const uint32_t expect = (b + 1 == nb) ? n - b * kAnsBlock : kAnsBlock;
       const uint32_t padded = (nw + 7) & ~7u;
       if (bs != expect || (uint64_t)pre + padded > cw || padded > kEncOutWords || (pre & 7)) {
         if (lane == 0) report_error(ctrl, MANS_ERR_CORRUPT, b);
+        b = nxt;
         continue;
       }
       // stage the block's words (16-byte aligned: over % 16 == 0, pre % 8 == 0)
       const uint4* src = reinterpret_cast<const uint4*>(data + 2ull * pre);
+      __syncwarp();
       for (uint32_t i = lane; i < padded / 8; i += 32) reinterpret_cast<uint4*>(sin)[i] = __ldg(src + i);
       __syncwarp();
-      uint8_t* dst = out + (uint64_t)b * kAnsBlock;
-      uint8_t* so = sout + phase16(dst);
+      uint8_t* dst = out + (uint64_t)b * kAnsBlock + lane;
       int ptr = (int)nw;
-      bool bad = false;
+      bool bad;
       const uint32_t rem = bs & 31;
       int j = (int)((bs + 31) >> 5) - 1;
       if (rem) {
         const bool valid = (uint32_t)lane < rem;
         if (valid) {
-          const uint32_t e = sm.lut[x & mask];
-          so[j * 32 + lane] = (uint8_t)e;
-          x = ((e >> 8) & 0xfffu) * (x >> p) + (e >> 20);
+          const uint32_t s0 = x & mask;
+          const uint32_t e = sm.lut[s0];
+          dst[j * 32] = sm.sym[s0];
+          x = (e >> 16) * (x >> p) + (e & 0xffffu);
         }
         const bool rd = valid && x < kAnsStartState;
         const uint32_t vote = __ballot_sync(0xffffffffu, rd);
-        if (rd) {
-          const int idx = ptr - __popc(vote & gemask);
-          if (idx >= 0) x = (x << 16) | sin[idx]; else bad = true;
-        }
+        if (rd) x = x * 65536u + sin[max(ptr - __popc(vote & gemask), 0)];
         ptr -= __popc(vote);
         --j;
       }
 #pragma unroll 4
       for (; j >= 0; --j) {
-        const uint32_t e = sm.lut[x & mask];
-        so[j * 32 + lane] = (uint8_t)e;
-        x = ((e >> 8) & 0xfffu) * (x >> p) + (e >> 20);
+        const uint32_t s0 = x & mask;
+        const uint32_t e = sm.lut[s0];
+        dst[j * 32] = sm.sym[s0];
+        x = (e >> 16) * (x >> p) + (e & 0xffffu);
         const bool rd = x < kAnsStartState;
         const uint32_t vote = __ballot_sync(0xffffffffu, rd);
-        if (rd) {
-          const int idx = ptr - __popc(vote & gemask);
-          if (idx >= 0) x = (x << 16) | sin[idx]; else bad = true;
-        }
+        // A read below the block's first word only happens in a corrupt
+        // stream; it is clamped here and caught by the final ptr check.
+        if (rd) x = x * 65536u + sin[max(ptr - __popc(vote & gemask), 0)];
         ptr -= __popc(vote);
       }
-      bad = bad || ptr != 0 || x != kAnsStartState;
+      bad = ptr != 0 || x != kAnsStartState;
       if (__any_sync(0xffffffffu, bad) && lane == 0) report_error(ctrl, MANS_ERR_CORRUPT, b);
-      __syncwarp();
-      warp_store_phase(dst, sout, bs, lane);
-      __syncwarp();
+      b = nxt;
     }
   }
 
@@ -377,11 +443,13 @@ static int occupancy(const void* fn, int threads, size_t smem) {
 }
 
 void init_ans_launch_cfg(LaunchCfg& cfg) {
-  cudaFuncSetAttribute(ans_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(ans_encode_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(EncSmem));
   cudaFuncSetAttribute(ans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(DecSmem));
-  cfg.enc_ctas = occupancy((const void*)ans_encode_kernel, kEncThreads, sizeof(EncSmem));
+  cfg.enc_ctas = occupancy((const void*)ans_encode_kernel<false>, kEncThreads, sizeof(EncSmem));
+  cfg.enc_slot_ctas = occupancy((const void*)ans_encode_kernel<true>, kEncThreads,
+                                sizeof(EncSmemTableOnly));
   cfg.dec_ctas = occupancy((const void*)ans_decode_kernel, kDecThreads, sizeof(DecSmem));
   cfg.hist_ctas = occupancy((const void*)hist_bytes_kernel, kHistThreads, 0);
 }
@@ -395,16 +463,27 @@ cudaError_t launch_hist_bytes(const uint8_t* in, uint64_t n, Ctrl* ctrl, int pro
   return cudaGetLastError();
 }
 
+uint64_t ans_encode_slot_bytes(const LaunchCfg& cfg) {
+  return (uint64_t)cfg.sms * cfg.enc_slot_ctas * kEncWarps * kEncSlotBytes;
+}
+
 cudaError_t launch_ans_encode(const uint8_t* in, uint8_t* out, uint64_t out_cap,
                               unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
                               unsigned long long* flags, uint32_t epoch, int prob_bits,
-                              uint64_t max_blocks, const LaunchCfg& cfg, cudaStream_t s) {
-  uint64_t want = div_up_u64(max_blocks, kEncWarps);
-  uint64_t cap = (uint64_t)cfg.sms * cfg.enc_ctas;
-  unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
-  ans_encode_kernel<<<grid, kEncThreads, sizeof(EncSmem), s>>>(in, out, out_cap, out_size64,
-                                                                out_size32, ctrl, flags, epoch,
-                                                                prob_bits);
+                              uint64_t max_blocks, const LaunchCfg& cfg, cudaStream_t s,
+                              uint8_t* slots) {
+  const uint64_t want = div_up_u64(max_blocks, kEncWarps);
+  if (slots) {
+    const uint64_t cap = (uint64_t)cfg.sms * cfg.enc_slot_ctas;
+    const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+    ans_encode_kernel<true><<<grid, kEncThreads, sizeof(EncSmemTableOnly), s>>>(
+        in, out, out_cap, out_size64, out_size32, ctrl, flags, epoch, prob_bits, slots);
+  } else {
+    const uint64_t cap = (uint64_t)cfg.sms * cfg.enc_ctas;
+    const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+    ans_encode_kernel<false><<<grid, kEncThreads, sizeof(EncSmem), s>>>(
+        in, out, out_cap, out_size64, out_size32, ctrl, flags, epoch, prob_bits, nullptr);
+  }
   return cudaGetLastError();
 }
 

@@ -96,6 +96,6 @@ extern "C" mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_i
   cudaError_t e = launch_hist_bytes(d_in, in_size, ctrl, precision, cfg, s);
   if (e == cudaSuccess)
     e = launch_ans_encode(d_in, d_out, ans_bound_bytes(in_size), nullptr, d_out_size, ctrl, flags,
-                          epoch, precision, div_up_u64(in_size, kAnsBlock), cfg, s);
+                          epoch, precision, div_up_u64(in_size, kAnsBlock), cfg, s, nullptr);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
 }

@@ -40,6 +40,7 @@ struct mans_workspace {
   unsigned long long* ans_flags = nullptr;
   uint64_t ans_flags_n = 0;
   uint8_t* merged = nullptr;  // 16-byte aligned region of merged_cap + slack bytes
+  uint8_t* enc_slots = nullptr;  // per-warp word slots of the encode kernel
   uint32_t epoch = 0;
   LaunchCfg cfg;
   // Opt-in kernel timing: a ring of event triples per recorded call
@@ -126,21 +127,23 @@ mans_status mans_workspace_create(mans_workspace** out, uint64_t max_input_bytes
   }
   ws->max_input_bytes = max_input_bytes;
   ws->merged_cap = merged_capacity;
-  // tiles of 4096 elements (ADM) and blocks of 4096 bytes (rANS)
-  ws->adm_flags_n = max_input_bytes / 8192 + 2;
+  // one flag per ADM group (512 elements, >= 1 KiB of input) and per 4 KiB rANS block
+  ws->adm_flags_n = max_input_bytes / 1024 + 2;
   uint64_t ans_src = merged_capacity > max_input_bytes ? merged_capacity : max_input_bytes;
   ws->ans_flags_n = div_up_u64(ans_src, kAnsBlock) + 2;
+  init_launch_cfg(ws->cfg, ws->device);
   const uint64_t off_ctrl = 0;
   const uint64_t off_adm = align_up(sizeof(Ctrl), 256);
   const uint64_t off_ans = align_up(off_adm + 8 * ws->adm_flags_n, 256);
-  const uint64_t off_m = align_up(off_ans + 8 * ws->ans_flags_n, 256);
+  const uint64_t off_slots = align_up(off_ans + 8 * ws->ans_flags_n, 256);
+  const uint64_t off_m = align_up(off_slots + ans_encode_slot_bytes(ws->cfg), 256);
   ws->bytes = align_up(off_m + merged_capacity + kSlack, 256);
   if (cudaMalloc(&ws->base, ws->bytes) != cudaSuccess) {
     cudaGetLastError();
     delete ws;
     return MANS_ERR_OUT_OF_MEMORY;
   }
-  if (cudaMemset(ws->base, 0, off_m) != cudaSuccess) {
+  if (cudaMemset(ws->base, 0, off_slots) != cudaSuccess) {
     cudaFree(ws->base);
     delete ws;
     return MANS_ERR_CUDA;
@@ -148,8 +151,8 @@ mans_status mans_workspace_create(mans_workspace** out, uint64_t max_input_bytes
   ws->ctrl = reinterpret_cast<Ctrl*>(ws->base + off_ctrl);
   ws->adm_flags = reinterpret_cast<unsigned long long*>(ws->base + off_adm);
   ws->ans_flags = reinterpret_cast<unsigned long long*>(ws->base + off_ans);
+  ws->enc_slots = ws->base + off_slots;
   ws->merged = ws->base + off_m;
-  init_launch_cfg(ws->cfg, ws->device);
   *out = ws;
   return MANS_OK;
 }
@@ -223,7 +226,7 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
     if (e == cudaSuccess)
       e = launch_ans_encode((const uint8_t*)d_in, (uint8_t*)d_out, out_capacity, osz, nullptr,
                             ws->ctrl, ws->ans_flags, epoch, precision,
-                            div_up_u64(in_bytes, kAnsBlock), ws->cfg, s);
+                            div_up_u64(in_bytes, kAnsBlock), ws->cfg, s, ws->enc_slots);
   } else if (dtype == MANS_U16) {
     const uint64_t hdr = adm_u16_header_bytes(n_elems);
     const uint64_t g = div_up_u64(n_elems, kAdmGroup);
@@ -235,7 +238,7 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
     if (e == cudaSuccess)
       e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
                             ws->ans_flags, epoch, precision,
-                            div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+                            div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s, ws->enc_slots);
   } else {
     const uint64_t hdr = adm_u32_header_bytes(n_elems);
     if (hdr + n_elems > ws->merged_cap) return MANS_ERR_TOO_LARGE;
@@ -246,7 +249,7 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
     if (e == cudaSuccess)
       e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
                             ws->ans_flags, epoch, precision,
-                            div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+                            div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s, ws->enc_slots);
   }
   mark(ws, 2, s);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
@@ -395,7 +398,7 @@ mans_status mans_ans_encode(int precision, const uint8_t* d_in, uint32_t in_size
   if (e == cudaSuccess)
     e = launch_ans_encode(d_in, d_out, ans_bound(in_size), nullptr, d_out_size, ws->ctrl,
                           ws->ans_flags, epoch, precision, div_up_u64(in_size, kAnsBlock),
-                          ws->cfg, s);
+                          ws->cfg, s, ws->enc_slots);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
 }
 

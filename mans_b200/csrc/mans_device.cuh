@@ -33,7 +33,7 @@ __host__ __device__ constexpr uint64_t ans_overhead(uint64_t nb) {
 constexpr int kAdmChunk = 16;     // elements per lane
 constexpr int kAdmGroup = 512;    // elements per group (one warp)
 constexpr uint32_t kAdmStep = 126;
-constexpr int kAdmGroupsPerTile = 8;  // one CTA of 8 warps maps 8 groups per tile
+constexpr int kAdmGroupsPerTile = 8;  // warps (groups in flight) per CTA of the mappers
 
 // ---- device status (first error wins) ----
 struct Ctrl {
@@ -70,13 +70,30 @@ __device__ __forceinline__ uint32_t lanemask_ge() {
   return m;
 }
 
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+// Look-back flags carry their own value, so they need coherence but no
+// ordering with other memory: relaxed GPU-scope accesses, no fences.
+__device__ __forceinline__ unsigned long long ld_flag(const unsigned long long* p) {
   unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ void st_flag(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Prefetch one 128-byte line into L1.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// Prefetch [p, p+bytes) into L2 with one bulk request (p and bytes are
+// rounded out to 16-byte boundaries; the range must lie in one allocation).
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(15);
+  const uintptr_t a1 = (reinterpret_cast<uintptr_t>(p) + bytes + 15) & ~uintptr_t(15);
+  if (a1 > a0)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"((uint32_t)(a1 - a0))
+                 : "memory");
 }
 
 // ---- single-pass decoupled look-back (epoch tagged, bounded waits) ----
@@ -89,8 +106,8 @@ __device__ __forceinline__ unsigned long long make_flag(uint32_t state, uint32_t
   return ((unsigned long long)value << 32) | ((unsigned long long)(epoch & 0x3fffffffu) << 2) |
          state;
 }
-// Bounded spin: about one second at most (2^20 polls x ~1 us backoff).
-constexpr uint32_t kSpinLimit = 1u << 20;
+// Bounded spin: about one second at most (2^22 polls x ~0.25 us backoff).
+constexpr uint32_t kSpinLimit = 1u << 22;
 
 // Warp-cooperative exclusive prefix of `tile` over flags[0..tile). Every lane
 // returns the same value. On timeout reports MANS_ERR_TIMEOUT and returns the
@@ -108,7 +125,7 @@ __device__ __forceinline__ uint32_t lookback_exclusive(unsigned long long* flags
     if (idx >= 0) {
       uint32_t spins = 0, ns = 32;
       while (true) {
-        w = ld_acquire_u64(&flags[idx]);
+        w = ld_flag(&flags[idx]);
         st = (uint32_t)(w & 3u);
         uint32_t wep = (uint32_t)((w >> 2) & 0x3fffffffu);
         if (st != 0 && wep == ep) break;
@@ -123,7 +140,7 @@ __device__ __forceinline__ uint32_t lookback_exclusive(unsigned long long* flags
           break;
         }
         __nanosleep(ns);
-        if (ns < 1024) ns <<= 1;
+        if (ns < 256) ns <<= 1;
       }
       val = (uint32_t)(w >> 32);
     }

@@ -11,7 +11,8 @@ struct Ctrl;
 
 struct LaunchCfg {
   int sms = 148;        // multiprocessors of the device
-  int enc_ctas = 0;     // resident CTAs per SM of the encode kernel
+  int enc_ctas = 0;     // resident CTAs per SM of the encode kernel (shared-memory staging)
+  int enc_slot_ctas = 0;  // resident CTAs per SM of the encode kernel (global slots)
   int dec_ctas = 0;     // resident CTAs per SM of the decode kernel
   int map_ctas = 0;     // resident CTAs per SM of the ADM map kernels
   int hist_ctas = 0;    // resident CTAs per SM of the byte histogram kernel
@@ -26,10 +27,14 @@ cudaError_t launch_hist_bytes(const uint8_t* in, uint64_t n, Ctrl* ctrl, int pro
                               const LaunchCfg& cfg, cudaStream_t s);
 // Encode ctrl->merged_size bytes at `in` (table from ctrl) into the coalesced
 // stream at `out`. max_blocks bounds the number of 4 KiB blocks (grid size).
+// slots: ans_encode_slot_bytes(cfg) bytes of global scratch for the words of
+// blocks in flight, or nullptr to compact them in shared memory instead.
 cudaError_t launch_ans_encode(const uint8_t* in, uint8_t* out, uint64_t out_cap,
                               unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
                               unsigned long long* flags, uint32_t epoch, int prob_bits,
-                              uint64_t max_blocks, const LaunchCfg& cfg, cudaStream_t s);
+                              uint64_t max_blocks, const LaunchCfg& cfg, cudaStream_t s,
+                              uint8_t* slots);
+uint64_t ans_encode_slot_bytes(const LaunchCfg& cfg);
 // Decode the stream at `in` into `out` (at most out_cap bytes). expect_p < 0
 // accepts any valid precision. record != 0 stores the decoded size in ctrl.
 cudaError_t launch_ans_decode(const uint8_t* in, uint64_t in_size, uint8_t* out, uint64_t out_cap,
