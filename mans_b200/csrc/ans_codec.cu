@@ -60,10 +60,10 @@ __global__ __launch_bounds__(kHistThreads) void hist_bytes_kernel(const uint8_t*
 // ------------------------------------------------------------------------
 // Encode (GpuANSEncode.h:25-164 arithmetic, :181-284 layout).
 //
-// One warp encodes one 4 KiB block: lane l codes bytes l, l+32, ... Symbols
-// are read straight from global memory, eight steps ahead of use, from lines
-// prefetched into L1 at the block's start and into L2 one grid of warps
-// earlier. Output words are compacted in a per-warp shared buffer (the
+// One warp encodes one 4 KiB block: lane l codes bytes l, l+32, ... The
+// block arrives in the warp's shared stage with one bulk (TMA) copy from L2,
+// where it was prefetched one grid of warps earlier; symbols are read eight
+// steps ahead of use. Output words are compacted in a per-warp shared buffer (the
 // only shared staging), then stored as 16-byte vectors once the block's word
 // offset is known.
 // ------------------------------------------------------------------------
@@ -73,12 +73,18 @@ constexpr uint32_t kEncOutWords = kAnsMaxBlockWords + 8;
 // A block's words compacted in global memory: slots of whole 128-byte lines.
 constexpr uint32_t kEncSlotBytes = (kEncOutWords * 2 + 127) / 128 * 128;
 
-struct EncSmem {
+constexpr uint32_t kEncStageBytes = kAnsBlock + 16;  // a block plus its 16-byte phase
+
+struct EncSmemSlots {  // words go to global slots
   uint2 table[kAnsSyms];
-  alignas(16) uint16_t out[kEncWarps][kEncOutWords];
+  alignas(16) uint8_t in[kEncWarps][kEncStageBytes];
+  uint64_t bar[kEncWarps];
 };
-struct EncSmemTableOnly {
+struct EncSmem {  // words compacted in shared memory
   uint2 table[kAnsSyms];
+  alignas(16) uint8_t in[kEncWarps][kEncStageBytes];
+  uint64_t bar[kEncWarps];
+  alignas(16) uint16_t out[kEncWarps][kEncOutWords];
 };
 
 // One interleaved step: renormalise (emit 16 bits, lanes in ascending order
@@ -122,11 +128,16 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
     unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
     unsigned long long* flags, uint32_t epoch, int p, uint8_t* __restrict__ slots) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  uint2* table = reinterpret_cast<uint2*>(smem_raw);
+  EncSmemSlots& ss = *reinterpret_cast<EncSmemSlots*>(smem_raw);  // common prefix of both layouts
+  uint2* table = ss.table;
   __shared__ int s_last;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const uint32_t ltmask = lanemask_lt();
   const uint32_t mp = 1u << p, sh = kAnsStateBits - p;
+  uint8_t* stage = ss.in[warp];
+  uint64_t* bar = &ss.bar[warp];
+  if (lane == 0) mbar_init(bar);
+  uint32_t parity = 0;
 
   const bool failed = *((volatile uint32_t*)&ctrl->status) != 0;
   const uint64_t n = __ldcg(&ctrl->merged_size);
@@ -175,8 +186,17 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
     }
     const uint64_t start = (uint64_t)b * kAnsBlock;
     const uint32_t bs = (uint32_t)min_u64(kAnsBlock, n - start);
-    const uint8_t* syms = in + start + lane;
-    if ((uint32_t)lane * 128 < bs) prefetch_l1(in + start + 128 * lane);
+    // one bulk copy of the block (rounded out to 16-byte boundaries) into this
+    // warp's stage; the previous block's reads of the stage are complete
+    __syncwarp();
+    if (lane == 0) {
+      const uintptr_t a0 = reinterpret_cast<uintptr_t>(in + start) & ~uintptr_t(15);
+      const uintptr_t a1 = (reinterpret_cast<uintptr_t>(in + start) + bs + 15) & ~uintptr_t(15);
+      bulk_load(stage, reinterpret_cast<const void*>(a0), (uint32_t)(a1 - a0), bar);
+    }
+    if (!mbar_wait(bar, parity) && lane == 0) report_error(ctrl, MANS_ERR_TIMEOUT, b);
+    parity ^= 1u;
+    const uint8_t* syms = stage + phase16(in + start) + lane;
 
     uint32_t x = kAnsStartState, nw = 0;
     const uint32_t full = bs >> 5;
@@ -184,11 +204,11 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
     if (full >= 8) {
       uint32_t cur[8];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) cur[u] = __ldg(syms + u * 32);
+      for (int u = 0; u < 8; ++u) cur[u] = syms[u * 32];
       for (; j + 16 <= full; j += 8) {
         uint32_t nx[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) nx[u] = __ldg(syms + (j + 8 + u) * 32);
+        for (int u = 0; u < 8; ++u) nx[u] = syms[(j + 8 + u) * 32];
 #pragma unroll
         for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
 #pragma unroll
@@ -198,10 +218,10 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
       for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
       j += 8;
     }
-    for (; j < full; ++j) enc_step(true, x, __ldg(syms + j * 32), table, sout, nw, mp, sh, ltmask);
+    for (; j < full; ++j) enc_step(true, x, syms[j * 32], table, sout, nw, mp, sh, ltmask);
     if (bs & 31) {
       const bool valid = (uint32_t)lane < (bs & 31);
-      enc_step(valid, x, valid ? __ldg(syms + j * 32) : 0u, table, sout, nw, mp, sh, ltmask);
+      enc_step(valid, x, valid ? syms[j * 32] : 0u, table, sout, nw, mp, sh, ltmask);
     }
 
     // Pad the word count to a 16-byte multiple with zeros (GpuANSEncode.h:275).
@@ -290,6 +310,7 @@ struct DecSmem {
   uint32_t lut[1 << kMaxProbBits];
   uint8_t sym[1 << kMaxProbBits];
   alignas(16) uint16_t in[kDecWarps][kEncOutWords];
+  uint64_t bar[kDecWarps];
 };
 
 __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
@@ -300,6 +321,9 @@ __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
   __shared__ uint32_t s_scan[kDecWarps];
   __shared__ int s_ok, s_last;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  uint64_t* bar = &sm.bar[warp];
+  if (lane == 0) mbar_init(bar);
+  uint32_t parity = 0;
 
   // ---- header validation (GpuANSCodec.h:106-113 asserts, GpuANSDecode.h:220-227)
   uint32_t h[5] = {0, 0, 0, 0, 0};
@@ -378,11 +402,14 @@ __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
         b = nxt;
         continue;
       }
-      // stage the block's words (16-byte aligned: over % 16 == 0, pre % 8 == 0)
-      const uint4* src = reinterpret_cast<const uint4*>(data + 2ull * pre);
+      // stage the block's words with one bulk copy (16-byte aligned: over % 16
+      // == 0, pre % 8 == 0); the previous block's reads of the stage are done
       __syncwarp();
-      for (uint32_t i = lane; i < padded / 8; i += 32) reinterpret_cast<uint4*>(sin)[i] = __ldg(src + i);
-      __syncwarp();
+      if (padded) {
+        if (lane == 0) bulk_load(sin, data + 2ull * pre, 2 * padded, bar);
+        if (!mbar_wait(bar, parity) && lane == 0) report_error(ctrl, MANS_ERR_TIMEOUT, b);
+        parity ^= 1u;
+      }
       uint8_t* dst = out + (uint64_t)b * kAnsBlock + lane;
       int ptr = (int)nw;
       bool bad;
@@ -448,8 +475,10 @@ void init_ans_launch_cfg(LaunchCfg& cfg) {
   cudaFuncSetAttribute(ans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(DecSmem));
   cfg.enc_ctas = occupancy((const void*)ans_encode_kernel<false>, kEncThreads, sizeof(EncSmem));
+  cudaFuncSetAttribute(ans_encode_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(EncSmemSlots));
   cfg.enc_slot_ctas = occupancy((const void*)ans_encode_kernel<true>, kEncThreads,
-                                sizeof(EncSmemTableOnly));
+                                sizeof(EncSmemSlots));
   cfg.dec_ctas = occupancy((const void*)ans_decode_kernel, kDecThreads, sizeof(DecSmem));
   cfg.hist_ctas = occupancy((const void*)hist_bytes_kernel, kHistThreads, 0);
 }
@@ -476,7 +505,7 @@ cudaError_t launch_ans_encode(const uint8_t* in, uint8_t* out, uint64_t out_cap,
   if (slots) {
     const uint64_t cap = (uint64_t)cfg.sms * cfg.enc_slot_ctas;
     const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
-    ans_encode_kernel<true><<<grid, kEncThreads, sizeof(EncSmemTableOnly), s>>>(
+    ans_encode_kernel<true><<<grid, kEncThreads, sizeof(EncSmemSlots), s>>>(
         in, out, out_cap, out_size64, out_size32, ctrl, flags, epoch, prob_bits, slots);
   } else {
     const uint64_t cap = (uint64_t)cfg.sms * cfg.enc_ctas;

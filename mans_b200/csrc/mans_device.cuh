@@ -96,6 +96,48 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
                  : "memory");
 }
 
+// ---- bulk (TMA) copies global -> shared with mbarrier completion ----
+// One mbarrier per warp-owned staging buffer, arrival count 1 (the issuing
+// lane). No multicast: each copy lands in the issuing CTA only.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Issued by one lane: copy `bytes` (multiple of 16; both addresses 16-byte
+// aligned) and arm the barrier's transaction count.
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gmem_src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(smem_dst)),
+      "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+// Bounded wait for the phase with the given parity to complete. Returns false
+// after 2^20 polls (each try_wait may suspend briefly; about a second at
+// most) and the caller records MANS_ERR_TIMEOUT.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_addr(bar);
+  for (uint32_t i = 0; i < (1u << 20); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // ---- single-pass decoupled look-back (epoch tagged, bounded waits) ----
 // A flag word packs {value:32}{epoch:30}{state:2}; state 1 = aggregate
 // published, 2 = inclusive prefix published. Flags from an older call carry
