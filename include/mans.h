@@ -139,6 +139,61 @@ mans_status mans_ans_last_status(mans_stream_t stream, uint64_t* detail);
 mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_in, uint32_t in_size,
                                     uint8_t* d_out, uint32_t* d_out_size, mans_stream_t stream);
 
+/* ------------------------------------------------------------------------
+ * Batched MANS: many buffers of uneven size and element type in one
+ * persistent launch per stage (a device work queue over every buffer's
+ * mapping groups and rANS blocks). Each buffer's stream is byte-identical to
+ * mans_compress of that buffer alone; errors are kept per buffer. The
+ * reference codes one buffer per call (examples/compress.cu:55-97 loops over
+ * files, src/GpuANS.cu:16-48 over whole inputs). Calls on one batch workspace
+ * must be ordered (one stream). Every call's bounds live on the device, so a
+ * call can be captured in a CUDA graph and replayed: each capture keeps its
+ * descriptors in the next of four host buffers, so the graphs of a
+ * workspace's last four captures may be replayed.
+ * ---------------------------------------------------------------------- */
+typedef struct mans_batch mans_batch;
+
+typedef struct mans_batch_item {
+  mans_dtype dtype;
+  int precision;          /* compress: probability bits, 9..11 */
+  uint64_t n_elems;       /* elements of the uncompressed buffer */
+  const void* d_in;       /* compress: values; decompress: stream (16-byte aligned) */
+  void* d_out;            /* compress: stream; decompress: values (16-byte aligned) */
+  uint64_t* d_out_size;   /* compress: device u64 receiving the stream size (may be NULL) */
+  uint64_t in_bytes;      /* decompress: stream bytes available at d_in */
+  uint64_t out_capacity;  /* compress: bytes available at d_out */
+} mans_batch_item;
+
+/* Workspace for batches of up to max_items buffers totalling at most
+ * max_total_bytes uncompressed bytes (on the current device). Each MANS_U16 /
+ * MANS_U32 buffer gets room for merged_ratio_pct percent of its bytes of
+ * mapped data, plus 4 KiB (0 = 210, the single-buffer default, enough for
+ * any MANS_U32 input); a buffer whose mapping needs more fails alone with
+ * MANS_ERR_WORKSPACE_OVERFLOW. */
+mans_status mans_batch_create(mans_batch** b, uint32_t max_items, uint64_t max_total_bytes,
+                              uint32_t merged_ratio_pct);
+mans_status mans_batch_destroy(mans_batch* b);
+uint64_t mans_batch_device_bytes(const mans_batch* b);
+/* Enqueue on `stream`; host-side argument errors are returned at once. */
+mans_status mans_batch_compress(mans_batch* b, const mans_batch_item* items, uint32_t count,
+                                mans_stream_t stream);
+mans_status mans_batch_decompress(mans_batch* b, const mans_batch_item* items, uint32_t count,
+                                  mans_stream_t stream);
+/* Synchronise `stream`; return the batch's first device-side error and fill
+ * the first `count` buffers' statuses and details (either may be NULL). */
+mans_status mans_batch_status(mans_batch* b, mans_stream_t stream, uint32_t* item_status,
+                              uint64_t* item_detail, uint32_t count);
+/* Schedule: resident CTAs per SM of each stage (map, plan, encode,
+ * decode plan, decode, unmap); never changes the bytes produced. */
+mans_status mans_batch_get_schedule(const mans_batch* b, int ctas_per_sm[6],
+                                    int max_ctas_per_sm[6]);
+mans_status mans_batch_set_schedule(mans_batch* b, const int ctas_per_sm[6]);
+/* Time candidate schedules on this batch (it is compressed several times),
+ * keep the fastest whose streams match the default schedule's checksum, and
+ * report its time. */
+mans_status mans_batch_autotune(mans_batch* b, const mans_batch_item* items, uint32_t count,
+                                mans_stream_t stream, float* best_ms);
+
 /* Library version string. */
 const char* mans_version(void);
 

@@ -54,6 +54,15 @@ SIGNATURES = {
     "mans_ans_max_compressed_size": (_u32, [_u32]),
     "mans_ans_last_status": (_i32, [_vp, C.POINTER(_u64)]),
     "mans_ans_encode_noalloc": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
+    "mans_batch_create": (_i32, [C.POINTER(_vp), _u32, _u64, _u32]),
+    "mans_batch_destroy": (_i32, [_vp]),
+    "mans_batch_device_bytes": (_u64, [_vp]),
+    "mans_batch_compress": (_i32, [_vp, _vp, _u32, _vp]),
+    "mans_batch_decompress": (_i32, [_vp, _vp, _u32, _vp]),
+    "mans_batch_status": (_i32, [_vp, _vp, C.POINTER(_u32), C.POINTER(_u64), _u32]),
+    "mans_batch_get_schedule": (_i32, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "mans_batch_set_schedule": (_i32, [_vp, C.POINTER(C.c_int)]),
+    "mans_batch_autotune": (_i32, [_vp, _vp, _u32, _vp, C.POINTER(C.c_float)]),
     "mans_version": (C.c_char_p, []),
     "mans_debug_enc_entry": (None, [_u32, _u32, _i32, C.POINTER(_u32)]),
 }

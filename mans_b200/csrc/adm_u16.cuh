@@ -1,0 +1,316 @@
+// adm_u16.cuh -- ADM byte mapping of uint16 arrays (unary bit-signal format)
+// for sm_100a: the per-group work of the map (fused with the group-length scan
+// and the rANS histogram) and of the unmap, shared by the single-buffer and
+// batched kernels.
+//
+// Format: mapping/nv/mappingV15_fused_uint16.cu (map :124-373 / :400-730,
+// merged layout :933-957), identical in its bytes to
+// mapping/cpu/mappingcpuV2.cpp:35-143. Per group of 512 elements (32 lanes x
+// 16 consecutive elements):
+//   center = truncated mean; code = 1 (center), 2r (above), 2r+1 (below) with
+//   r = d - 126(k-1), k = ceil(d/126); each element appends "1" then k-1 "0"s
+//   to its lane's bit stream (MSB first); the group length L is the longest
+//   lane in bytes; a shorter lane's final partial byte is filled with 1s.
+// Merged: [i32 exclusive L prefix x g][u16 center x g][u8 code x n][bits].
+//
+// B200 organisation: each warp maps one group at a time, groups handed out
+// in order by an atomic counter. The group-length prefix is a single-pass
+// decoupled look-back over per-group flags (the reference V15 uses a thrust
+// scan plus a concat kernel above 1,024 groups, and an unbounded look-back
+// below), so bits are written once, directly at their final offset. Every
+// byte written is counted in a per-warp shared histogram, which gives the
+// rANS histogram of the merged buffer without reading it again.
+#pragma once
+
+#include "ans_table.cuh"
+
+namespace mans {
+
+constexpr int kMapWarps = kAdmGroupsPerTile;  // 8
+constexpr int kMapThreads = kMapWarps * 32;   // 256
+
+// floor(a / 126) for a < 89,240: (a * ceil(2^23/126)) >> 23.
+__device__ __forceinline__ uint32_t div126(uint32_t a) {
+  return __umulhi(a << 9, 66577u);
+}
+
+// k = max(1, ceil(d/126)), code = 2r + (v <= c), r = d + 126 - 126k.
+__device__ __forceinline__ void adm_elem_u16(uint32_t v, uint32_t c, uint32_t& k, uint32_t& code) {
+  const uint32_t d = (uint32_t)abs((int)v - (int)c);
+  k = max(1u, div126(d + 125u));
+  const uint32_t r = d + 126u - 126u * k;
+  code = 2u * r + (v <= c ? 1u : 0u);
+}
+
+__device__ __forceinline__ uint32_t elem16(const uint32_t (&w)[8], int i) {
+  return (w[i >> 1] >> ((i & 1) * 16)) & 0xffffu;
+}
+
+// Bits [63-(pos|7), 63-pos] set: the rest of the byte holding stream bit pos.
+__device__ __forceinline__ uint64_t tail_fill_mask(uint32_t pos) {
+  const uint64_t hi = (pos == 0) ? ~0ull : ((1ull << (64 - pos)) - 1);
+  const uint32_t lo_bits = 63 - (pos | 7);
+  const uint64_t lo = (1ull << lo_bits) - 1;
+  return hi & ~lo;
+}
+
+// Lane's 16 elements of group grp as 8 packed words (zeros past n).
+__device__ __forceinline__ void load_lane_u16(const uint16_t* __restrict__ in, uint64_t n,
+                                              uint64_t grp, int lane, uint32_t (&w)[8]) {
+  const uint64_t ls = grp * kAdmGroup + (uint64_t)lane * kAdmChunk;
+  if (ls + 16 <= n) {
+    const uint4* src = reinterpret_cast<const uint4*>(in + ls);
+    const uint4 a = __ldcs(src), b = __ldcs(src + 1);
+    w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+    w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint32_t lo = (ls + 2 * i < n) ? in[ls + 2 * i] : 0u;
+      const uint32_t hi = (ls + 2 * i + 1 < n) ? in[ls + 2 * i + 1] : 0u;
+      w[i] = lo | (hi << 16);
+    }
+  }
+}
+
+// Map group `grp` of one buffer (one warp). flags: the buffer's per-group
+// look-back flags; msize_out: written by the buffer's last group; hist: the
+// warp's shared histogram.
+__device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uint64_t n,
+                                            uint8_t* __restrict__ M, uint64_t m_cap,
+                                            unsigned long long* flags,
+                                            unsigned long long* msize_out, uint32_t grp,
+                                            uint32_t epoch, const Sink& sink, uint32_t* hist,
+                                            int lane) {
+  const uint64_t g = div_up_u64(n, kAdmGroup);
+  uint8_t* p_len = M;
+  uint8_t* p_ctr = M + 4 * g;
+  uint8_t* p_code = M + 6 * g;
+  uint8_t* p_bits = M + 6 * g + n;
+  const uint64_t bits_base = 6 * g + n;  // offset of the bits section in M
+  uint32_t w[8];
+  load_lane_u16(in, n, grp, lane, w);
+
+  const uint64_t gs = (uint64_t)grp * kAdmGroup;
+  const uint64_t ls = gs + (uint64_t)lane * kAdmChunk;
+  const int cnt = ls >= n ? 0 : (int)min_u64(16, n - ls);
+
+  // ---- center: truncated mean (u32 sum of at most 512 uint16 values)
+  uint32_t lsum = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) lsum += (w[i] & 0xffffu) + (w[i] >> 16);
+  const uint32_t gsum = __reduce_add_sync(0xffffffffu, lsum);
+  const uint32_t gcnt = (uint32_t)min_u64(kAdmGroup, n - gs);
+  const uint32_t c = gcnt == kAdmGroup ? (gsum >> 9) : gsum / gcnt;
+
+  // ---- map: codes, unary bits (first 64 bits in a register), lane length
+  uint32_t codes[4] = {0, 0, 0, 0};
+  uint64_t acc = 0;
+  uint32_t pos = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    if (i < cnt) {
+      uint32_t k, code;
+      adm_elem_u16(elem16(w, i), c, k, code);
+      codes[i >> 2] |= code << ((i & 3) * 8);
+      atomicAdd(&hist[code], 1u);
+      if (pos < 64) acc |= 0x8000000000000000ull >> pos;
+      pos += k;
+    }
+  }
+  const uint32_t L = __reduce_max_sync(0xffffffffu, (pos + 7) >> 3);
+
+  // ---- publish the group length now; the prefix is read after the work
+  //      that does not depend on it
+  if (lane == 0) st_flag(&flags[grp], make_flag(grp == 0 ? kFlagIncl : kFlagAgg, epoch, L));
+
+  // codes: 16-byte aligned (the codes section is aligned by the caller)
+  if (cnt == 16) {
+    *reinterpret_cast<uint4*>(p_code + ls) = make_uint4(codes[0], codes[1], codes[2], codes[3]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      if (i < cnt) p_code[ls + i] = (uint8_t)(codes[i >> 2] >> ((i & 3) * 8));
+  }
+  // bit bytes of a short lane (< 64 bits): tail fill and histogram now
+  const bool fast = pos < 64;
+  if (fast) {
+    if (pos < 8 * L) acc |= tail_fill_mask(pos);
+    const uint32_t nb8 = L < 8 ? L : 8u;
+    for (uint32_t b = 0; b < nb8; ++b) atomicAdd(&hist[(uint32_t)(acc >> (56 - 8 * b)) & 0xffu], 1u);
+    if (L > 8) atomicAdd(&hist[0], L - 8);
+  }
+
+  // ---- group bit offset (in units of 32 bytes)
+  uint32_t gexcl = 0;
+  if (grp > 0) {
+    gexcl = lookback_exclusive(flags, grp, epoch, sink);
+    if (lane == 0) st_flag(&flags[grp], make_flag(kFlagIncl, epoch, gexcl + L));
+  }
+  if (lane == 0 && (uint64_t)grp + 1 == g) {
+    const unsigned long long msize = bits_base + 32ull * (gexcl + L);
+    *msize_out = msize;
+    if (msize > m_cap) report(sink, MANS_ERR_WORKSPACE_OVERFLOW, msize);
+  }
+
+  // lengths (i32, written as two u16: M is only 2-byte aligned here) and center
+  if (lane == 0) {
+    reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[0] = (uint16_t)(gexcl & 0xffffu);
+    reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[1] = (uint16_t)(gexcl >> 16);
+    reinterpret_cast<uint16_t*>(p_ctr + 2ull * grp)[0] = (uint16_t)c;
+    atomicAdd(&hist[gexcl & 0xff], 1u);
+    atomicAdd(&hist[(gexcl >> 8) & 0xff], 1u);
+    atomicAdd(&hist[(gexcl >> 16) & 0xff], 1u);
+    atomicAdd(&hist[gexcl >> 24], 1u);
+    atomicAdd(&hist[c & 0xff], 1u);
+    atomicAdd(&hist[(c >> 8) & 0xff], 1u);
+  }
+  // bits: lane region [32*gexcl + lane*L, +L) of the bits section
+  const uint64_t gend = bits_base + 32ull * ((uint64_t)gexcl + L);
+  if (gend <= m_cap) {
+    uint8_t* dst = p_bits + 32ull * gexcl + (uint64_t)lane * L;
+    if (fast) {
+      for (uint32_t b = 0; b < L; ++b)
+        dst[b] = (uint8_t)(b < 8 ? (uint32_t)(acc >> (56 - 8 * b)) & 0xffu : 0u);
+    } else {
+      // Long lane: regenerate the stream byte by byte.
+      uint32_t cur = 0, bi = 0, bp = 0;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        if (i < cnt) {
+          uint32_t k, code;
+          adm_elem_u16(elem16(w, i), c, k, code);
+          while ((bp >> 3) > bi) {
+            dst[bi++] = (uint8_t)cur;
+            atomicAdd(&hist[cur], 1u);
+            cur = 0;
+          }
+          cur |= 0x80u >> (bp & 7);
+          bp += k;
+        }
+      }
+      while ((pos >> 3) > bi) {
+        dst[bi++] = (uint8_t)cur;
+        atomicAdd(&hist[cur], 1u);
+        cur = 0;
+      }
+      if (bi < L) {
+        if (pos < 8 * L) cur |= 0xffu >> (pos & 7);
+        dst[bi++] = (uint8_t)cur;
+        atomicAdd(&hist[cur], 1u);
+      }
+      for (; bi < L; ++bi) {
+        dst[bi] = 0;
+        atomicAdd(&hist[0], 1u);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Unmap: restore the lane signals (mappingcpuV2.cpp:161-197, V15 :39-86) and
+// values (mappingcpuV2.cpp:202-224, V15 :101-112). One warp per group.
+// ------------------------------------------------------------------------
+constexpr int kUnmapThreads = 256;
+
+__device__ __forceinline__ uint32_t rd_u32_2aligned(const uint8_t* p) {
+  const uint16_t* q = reinterpret_cast<const uint16_t*>(p);
+  return (uint32_t)q[0] | ((uint32_t)q[1] << 16);
+}
+
+// Restore group `grp` of one buffer (one warp). msize: the merged size
+// recorded by the decoder; tot: bit bytes / 32 (validated by the caller).
+__device__ __forceinline__ void unmap16_group(const uint8_t* __restrict__ M, uint64_t n,
+                                              uint64_t tot, uint16_t* __restrict__ out,
+                                              uint64_t grp, const Sink& sink, int lane) {
+  const uint64_t g = div_up_u64(n, kAdmGroup);
+  const uint64_t bits_base = 6 * g + n;
+  const uint8_t* p_len = M;
+  const uint8_t* p_ctr = M + 4 * g;
+  const uint8_t* p_code = M + 6 * g;
+  const uint8_t* p_bits = M + bits_base;
+  const uint64_t ex = rd_u32_2aligned(p_len + 4 * grp);
+  const uint64_t nx = grp + 1 < g ? rd_u32_2aligned(p_len + 4 * (grp + 1)) : tot;
+  if (ex > nx || nx > tot) {
+    if (lane == 0) report(sink, MANS_ERR_CORRUPT, grp);
+    return;
+  }
+  const uint32_t L = (uint32_t)(nx - ex);
+  const uint32_t c = reinterpret_cast<const uint16_t*>(p_ctr)[grp];
+  const uint64_t ls = grp * kAdmGroup + (uint64_t)lane * kAdmChunk;
+  const int cnt = ls >= n ? 0 : (int)min_u64(16, n - ls);
+  uint32_t codes[4] = {0, 0, 0, 0};
+  if (cnt == 16) {
+    const uint4 v = __ldcs(reinterpret_cast<const uint4*>(p_code + ls));
+    codes[0] = v.x; codes[1] = v.y; codes[2] = v.z; codes[3] = v.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      if (i < cnt) codes[i >> 2] |= (uint32_t)p_code[ls + i] << ((i & 3) * 8);
+  }
+  const uint8_t* src = p_bits + 32ull * ex + (uint64_t)lane * L;
+  uint32_t sig[16];
+  bool bad = false;
+  if (L <= 8) {
+    uint64_t acc = 0;
+    for (uint32_t b = 0; b < L; ++b) acc |= (uint64_t)src[b] << (56 - 8 * b);
+    const int nbits = 8 * (int)L;
+    int pos = 0;  // stream position of the current element's leading 1
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      sig[i] = 0;
+      if (i < cnt) {
+        if (pos >= nbits || !((acc << pos) >> 63)) bad = true;
+        const uint64_t rest = pos + 1 < 64 ? (acc << (pos + 1)) : 0ull;
+        int z = rest ? __clzll(rest) : 64;
+        const int left = nbits - pos - 1;
+        z = z < left ? z : (left > 0 ? left : 0);
+        sig[i] = (uint32_t)z;
+        pos += z + 1;
+      }
+    }
+  } else {
+    // Long lanes: scan byte by byte like the reference.
+    int idx = -1;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sig[i] = 0;
+    for (uint32_t b = 0; b < L && idx < 16; ++b) {
+      const uint32_t byte = src[b];
+      for (int bit = 7; bit >= 0 && idx < 16; --bit) {
+        if ((byte >> bit) & 1u) {
+          ++idx;
+        } else if (idx < 0) {
+          bad = true;
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) sig[i] += (i == idx) ? 1u : 0u;
+        }
+      }
+    }
+    if (idx < cnt - 1) bad = true;
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) report(sink, MANS_ERR_CORRUPT, grp);
+  uint32_t vals[8];
+#pragma unroll
+  for (int i = 0; i < 16; i += 2) {
+    uint32_t r[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t code = (codes[(i + h) >> 2] >> (((i + h) & 3) * 8)) & 0xffu;
+      const uint32_t d = (code >> 1) + 126u * sig[i + h];
+      r[h] = ((code & 1u) ? c - d : c + d) & 0xffffu;
+    }
+    vals[i >> 1] = r[0] | (r[1] << 16);
+  }
+  if (cnt == 16) {
+    uint4* o = reinterpret_cast<uint4*>(out + ls);
+    o[0] = make_uint4(vals[0], vals[1], vals[2], vals[3]);
+    o[1] = make_uint4(vals[4], vals[5], vals[6], vals[7]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      if (i < cnt) out[ls + i] = (uint16_t)(vals[i >> 1] >> ((i & 1) * 16));
+  }
+}
+
+}  // namespace mans

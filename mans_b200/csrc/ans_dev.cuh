@@ -1,0 +1,277 @@
+// ans_dev.cuh -- per-block work of the byte rANS codec for sm_100a (encode
+// with in-place output compaction, decode), shared by the single-buffer and
+// batched kernels.
+//
+// Arithmetic and layout: include/ans/GpuANSEncode.h:25-164 and :181-284,
+// include/ans/GpuANSDecode.h:27-302 (see ans_codec.cu for the organisation).
+#pragma once
+
+#include "ans_table.cuh"
+#include "smem_io.cuh"
+
+namespace mans {
+
+constexpr int kEncWarps = 8;
+constexpr int kEncThreads = kEncWarps * 32;
+constexpr uint32_t kEncOutWords = kAnsMaxBlockWords + 8;
+// A block's words compacted in global memory: slots of whole 128-byte lines.
+constexpr uint32_t kEncSlotBytes = (kEncOutWords * 2 + 127) / 128 * 128;
+
+constexpr uint32_t kEncStageBytes = kAnsBlock + 16;  // a block plus its 16-byte phase
+
+struct EncSmemSlots {  // words go to global slots
+  uint2 table[kAnsSyms];
+  alignas(16) uint8_t in[kEncWarps][kEncStageBytes];
+  uint64_t bar[kEncWarps];
+};
+struct EncSmem {  // words compacted in shared memory
+  uint2 table[kAnsSyms];
+  alignas(16) uint8_t in[kEncWarps][kEncStageBytes];
+  uint64_t bar[kEncWarps];
+  alignas(16) uint16_t out[kEncWarps][kEncOutWords];
+};
+
+// One interleaved step: renormalise (emit 16 bits, lanes in ascending order
+// into the compacted word buffer), then x = (x/pdf << p) + x%pdf + cdf.
+__device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
+                                         const uint2* __restrict__ tab, uint16_t* __restrict__ out,
+                                         uint32_t& nw, uint32_t mp, uint32_t sh, uint32_t ltmask) {
+  const uint2 e = tab[sym];
+  const uint32_t cmpl = (e.y >> 13) & 0xfffu;
+  const uint32_t thr = (mp - cmpl) << sh;
+  const bool wr = valid && x >= thr;
+  const uint32_t vote = __ballot_sync(0xffffffffu, wr);
+  if (wr) out[nw + __popc(vote & ltmask)] = (uint16_t)(x & 0xffffu);
+  nw += __popc(vote);
+  const uint32_t xr = wr ? (x >> 16) : x;
+  if (valid) {
+    const uint32_t q = __umulhi(xr, e.x) >> (e.y >> 25);
+    x = xr + (e.y & 0x1fffu) + q * cmpl;
+  } else {
+    x = xr;
+  }
+}
+
+__device__ __forceinline__ void discard_l2_line(const void* p) {
+  asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
+// Encode block b of one buffer (one warp) and store it at its place in the
+// coalesced stream; the buffer's last block also writes the header and pdf.
+// in / n: the bytes being coded; flags: the buffer's per-block look-back
+// flags; stage / bar / parity: the warp's bulk-copy stage; sout: the warp's
+// word buffer -- with kSlots a per-warp slot in global memory, which stays in
+// L2 and is discarded after the final copy (shared memory then holds only
+// the table and the stage), otherwise shared memory.
+template <bool kSlots>
+__device__ __forceinline__ void encode_block(
+    const uint8_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ out, uint64_t out_cap,
+    unsigned long long* out_size64, uint32_t* out_size32, const uint32_t* __restrict__ pdf,
+    unsigned long long* flags, uint32_t epoch, int p, const Sink& sink, const uint2* table,
+    uint8_t* stage, uint64_t* bar, uint32_t& parity, uint16_t* sout, uint32_t b, int lane) {
+  const uint32_t ltmask = lanemask_lt();
+  const uint32_t mp = 1u << p, sh = kAnsStateBits - p;
+  const uint64_t nb = div_up_u64(n, kAnsBlock);
+  const uint64_t over = ans_overhead(nb);
+  const uint64_t start = (uint64_t)b * kAnsBlock;
+  const uint32_t bs = (uint32_t)min_u64(kAnsBlock, n - start);
+  // one bulk copy of the block (rounded out to 16-byte boundaries) into this
+  // warp's stage; the previous block's reads of the stage are complete
+  __syncwarp();
+  if (lane == 0) {
+    const uintptr_t a0 = reinterpret_cast<uintptr_t>(in + start) & ~uintptr_t(15);
+    const uintptr_t a1 = (reinterpret_cast<uintptr_t>(in + start) + bs + 15) & ~uintptr_t(15);
+    bulk_load(stage, reinterpret_cast<const void*>(a0), (uint32_t)(a1 - a0), bar);
+  }
+  if (!mbar_wait(bar, parity) && lane == 0) report(sink, MANS_ERR_TIMEOUT, b);
+  parity ^= 1u;
+  const uint8_t* syms = stage + phase16(in + start) + lane;
+
+  uint32_t x = kAnsStartState, nw = 0;
+  const uint32_t full = bs >> 5;
+  uint32_t j = 0;
+  if (full >= 8) {
+    uint32_t cur[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) cur[u] = syms[u * 32];
+    for (; j + 16 <= full; j += 8) {
+      uint32_t nx[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) nx[u] = syms[(j + 8 + u) * 32];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) cur[u] = nx[u];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
+    j += 8;
+  }
+  for (; j < full; ++j) enc_step(true, x, syms[j * 32], table, sout, nw, mp, sh, ltmask);
+  if (bs & 31) {
+    const bool valid = (uint32_t)lane < (bs & 31);
+    enc_step(valid, x, valid ? syms[j * 32] : 0u, table, sout, nw, mp, sh, ltmask);
+  }
+
+  // Pad the word count to a 16-byte multiple with zeros (GpuANSEncode.h:275).
+  const uint32_t padded = (nw + 7) & ~7u;
+  if ((uint32_t)lane < padded - nw) sout[nw + lane] = 0;
+
+  // Single-pass prefix over padded word counts.
+  if (lane == 0) st_flag(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, padded));
+  uint32_t prefix = 0;
+  if (b > 0) {
+    prefix = lookback_exclusive(flags, b, epoch, sink);
+    if (lane == 0) st_flag(&flags[b], make_flag(kFlagIncl, epoch, prefix + padded));
+  }
+  __syncwarp();
+
+  const uint64_t end = over + 2ull * ((uint64_t)prefix + padded);
+  const bool last = (uint64_t)b + 1 == nb;
+  if (last && end > out_cap && lane == 0) report(sink, MANS_ERR_OUTPUT_OVERFLOW, end);
+  if (end <= out_cap) {
+    uint32_t* states = reinterpret_cast<uint32_t*>(out + kAnsHeaderBytes + 2 * kAnsSyms);
+    states[(uint64_t)b * 32 + lane] = x;
+    uint2* bw = reinterpret_cast<uint2*>(out + kAnsHeaderBytes + 2 * kAnsSyms + 128 * nb);
+    if (lane == 0) bw[b] = make_uint2((bs << 16) | nw, prefix);
+    uint4* dst = reinterpret_cast<uint4*>(out + over + 2ull * prefix);
+    const uint4* src = reinterpret_cast<const uint4*>(sout);
+    for (uint32_t i = lane; i < padded / 8; i += 32) {
+      if (kSlots) dst[i] = __ldcg(src + i);
+      else dst[i] = src[i];
+    }
+    if (last) {
+      if (lane < 8) {
+        const uint32_t hv = lane == 0 ? kAnsMagicVersion
+                          : lane == 1 ? (uint32_t)nb
+                          : lane == 2 ? (uint32_t)n
+                          : lane == 3 ? prefix + padded
+                          : lane == 4 ? (uint32_t)p : 0u;
+        reinterpret_cast<uint32_t*>(out)[lane] = hv;
+      }
+      for (int i = lane; i < kAnsSyms; i += 32)
+        reinterpret_cast<uint16_t*>(out + kAnsHeaderBytes)[i] = (uint16_t)pdf[i];
+      if (lane == 0 && (nb & 1)) bw[nb] = make_uint2(0, 0);
+      if (lane == 0) {
+        if (out_size64) *out_size64 = end;
+        if (out_size32) *out_size32 = (uint32_t)end;
+      }
+    }
+  }
+  __syncwarp();
+  if (kSlots) {
+    // the slot's lines are consumed: drop them from L2 without write-back
+    const uint32_t lines = (2 * padded + 127) / 128;
+    if ((uint32_t)lane < lines) discard_l2_line(reinterpret_cast<const uint8_t*>(sout) + 128 * lane);
+    if ((uint32_t)lane + 32 < lines)
+      discard_l2_line(reinterpret_cast<const uint8_t*>(sout) + 128 * (lane + 32));
+    __syncwarp();
+  }
+}
+
+constexpr int kDecWarps = 8;
+constexpr int kDecThreads = kDecWarps * 32;
+constexpr int kMaxProbBits = 11;
+
+// Build the slot tables of a stream's pdf in shared memory (one CTA of 256
+// threads, thread t owns symbol t): lut[s] = pdf << 16 | (s - cdf), sym[s] =
+// the symbol (GpuANSDecode.h:307-377 packs the same fields in one word).
+// Returns false when the pdf does not sum to 2^p.
+__device__ __forceinline__ bool build_decode_tables(const uint8_t* __restrict__ in, int p,
+                                                    uint32_t* lut, uint8_t* sym,
+                                                    uint32_t* s_scan) {
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const uint16_t* probs = reinterpret_cast<const uint16_t*>(in + kAnsHeaderBytes);
+  const uint32_t pdf = __ldg(probs + t);
+  uint32_t incl = pdf;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  __syncthreads();
+  if (lane == 31) s_scan[warp] = incl;
+  __syncthreads();
+  uint32_t base = 0, total = 0;
+  for (int w = 0; w < kDecWarps; ++w) {
+    if (w < warp) base += s_scan[w];
+    total += s_scan[w];
+  }
+  const uint32_t cdf = base + incl - pdf;
+  if (total != (1u << p)) return false;
+  for (uint32_t j = 0; j < pdf; ++j) {
+    lut[cdf + j] = (pdf << 16) | j;
+    sym[cdf + j] = (uint8_t)t;
+  }
+  return true;
+}
+
+// Decode block b of one stream (one warp) into out + 4096 b. in: the stream
+// (header validated by the caller: nb blocks, n bytes, cw words, precision
+// p); lut / sym: the slot tables; sin / bar / parity: the warp's word stage.
+__device__ __forceinline__ void decode_block(const uint8_t* __restrict__ in, uint32_t nb,
+                                             uint32_t n, uint32_t cw, int p,
+                                             uint8_t* __restrict__ out, const uint32_t* lut,
+                                             const uint8_t* sym, uint16_t* sin, uint64_t* bar,
+                                             uint32_t& parity, const Sink& sink, uint32_t b,
+                                             int lane) {
+  const uint64_t over = ans_overhead(nb);
+  const uint32_t* states = reinterpret_cast<const uint32_t*>(in + kAnsHeaderBytes + 2 * kAnsSyms);
+  const uint2* bwords = reinterpret_cast<const uint2*>(in + kAnsHeaderBytes + 2 * kAnsSyms + 128ull * nb);
+  const uint8_t* data = in + over;
+  const uint32_t mask = (1u << p) - 1u;
+  const uint32_t gemask = lanemask_ge();
+  uint32_t x = __ldg(states + (uint64_t)b * 32 + lane);
+  const uint2 bw = __ldg(bwords + b);
+  const uint32_t bs = bw.x >> 16, nw = bw.x & 0xffffu, pre = bw.y;
+  const uint32_t expect = (b + 1 == nb) ? n - b * kAnsBlock : kAnsBlock;
+  const uint32_t padded = (nw + 7) & ~7u;
+  if (bs != expect || (uint64_t)pre + padded > cw || padded > kEncOutWords || (pre & 7)) {
+    if (lane == 0) report(sink, MANS_ERR_CORRUPT, b);
+    return;
+  }
+  // stage the block's words with one bulk copy (16-byte aligned: over % 16
+  // == 0, pre % 8 == 0); the previous block's reads of the stage are done
+  __syncwarp();
+  if (padded) {
+    if (lane == 0) bulk_load(sin, data + 2ull * pre, 2 * padded, bar);
+    if (!mbar_wait(bar, parity) && lane == 0) report(sink, MANS_ERR_TIMEOUT, b);
+    parity ^= 1u;
+  }
+  uint8_t* dst = out + (uint64_t)b * kAnsBlock + lane;
+  int ptr = (int)nw;
+  bool bad;
+  const uint32_t rem = bs & 31;
+  int j = (int)((bs + 31) >> 5) - 1;
+  if (rem) {
+    const bool valid = (uint32_t)lane < rem;
+    if (valid) {
+      const uint32_t s0 = x & mask;
+      const uint32_t e = lut[s0];
+      dst[j * 32] = sym[s0];
+      x = (e >> 16) * (x >> p) + (e & 0xffffu);
+    }
+    const bool rd = valid && x < kAnsStartState;
+    const uint32_t vote = __ballot_sync(0xffffffffu, rd);
+    if (rd) x = x * 65536u + sin[max(ptr - __popc(vote & gemask), 0)];
+    ptr -= __popc(vote);
+    --j;
+  }
+#pragma unroll 4
+  for (; j >= 0; --j) {
+    const uint32_t s0 = x & mask;
+    const uint32_t e = lut[s0];
+    dst[j * 32] = sym[s0];
+    x = (e >> 16) * (x >> p) + (e & 0xffffu);
+    const bool rd = x < kAnsStartState;
+    const uint32_t vote = __ballot_sync(0xffffffffu, rd);
+    // A read below the block's first word only happens in a corrupt
+    // stream; it is clamped here and caught by the final ptr check.
+    if (rd) x = x * 65536u + sin[max(ptr - __popc(vote & gemask), 0)];
+    ptr -= __popc(vote);
+  }
+  bad = ptr != 0 || x != kAnsStartState;
+  if (__any_sync(0xffffffffu, bad) && lane == 0) report(sink, MANS_ERR_CORRUPT, b);
+}
+
+}  // namespace mans

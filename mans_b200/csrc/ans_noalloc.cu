@@ -12,8 +12,9 @@
 // library holds until the process exits. All calls on a device share it:
 // calls that overlap on the GPU (e.g. on two streams) race and must not be
 // issued; calls ordered on one stream are fine. Each call clears the part of
-// the array that must start at zero; the flags need no clearing because
-// every call tags them with a new epoch.
+// the array that must start at zero (status, counters, histogram); the flags
+// need no clearing because each call tags them with the epoch kept in the
+// control block, which the call's last kernel advances.
 #include <cstddef>
 #include <mutex>
 
@@ -35,7 +36,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 struct DeviceState {
   bool ready = false;
   unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
-  uint32_t epoch = 0;
   LaunchCfg cfg;
 };
 constexpr int kMaxDevices = 64;
@@ -66,7 +66,6 @@ extern "C" mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_i
   if (dev < 0 || dev >= kMaxDevices) return MANS_ERR_INVALID_ARG;
 
   unsigned char* scratch = nullptr;
-  uint32_t epoch = 0;
   LaunchCfg cfg;
   {
     std::lock_guard<std::mutex> lock(g_mu);
@@ -82,10 +81,7 @@ extern "C" mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_i
       init_launch_cfg(st.cfg, dev);
       st.ready = true;
     }
-    st.epoch = (st.epoch + 1) & 0x3fffffffu;
-    if (st.epoch == 0) st.epoch = 1;
     scratch = st.scratch;
-    epoch = st.epoch;
     cfg = st.cfg;
   }
   Ctrl* ctrl = reinterpret_cast<Ctrl*>(scratch);
@@ -96,6 +92,6 @@ extern "C" mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_i
   cudaError_t e = launch_hist_bytes(d_in, in_size, ctrl, precision, cfg, s);
   if (e == cudaSuccess)
     e = launch_ans_encode(d_in, d_out, ans_bound_bytes(in_size), nullptr, d_out_size, ctrl, flags,
-                          epoch, precision, div_up_u64(in_size, kAnsBlock), cfg, s, nullptr);
+                          precision, div_up_u64(in_size, kAnsBlock), cfg, s, nullptr);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
 }

@@ -1,0 +1,362 @@
+// batch_capi.cu -- C ABI of the batched codec (include/mans.h, "batch"):
+// workspace, per-call layout of the buffers, descriptor upload, status
+// read-back and the schedule autotuner.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "batch_internal.h"
+#include "mans_device.cuh"
+
+using namespace mans;
+
+namespace {
+constexpr int kStagingRing = 2;
+constexpr int kCaptureSlots = 4;
+constexpr uint64_t kItemSlack = 4096 + 64;
+constexpr uint64_t kMaxMerged = 0xfffffff0ull;  // rANS header counts are u32
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+inline uint64_t elem_bytes(uint32_t d) { return d == MANS_U8 ? 1 : d == MANS_U16 ? 2 : d == MANS_U32 ? 4 : 0; }
+// Mapped-byte capacity of one buffer: ratio_pct percent of its bytes (210 =
+// the single-buffer workspace's default) plus one rANS block.
+inline uint64_t mapped_cap(uint64_t bytes, uint32_t ratio_pct) {
+  return bytes / 100 * ratio_pct + (bytes % 100) * ratio_pct / 100 + 4096;
+}
+}  // namespace
+
+struct mans_batch {
+  int device = 0;
+  uint32_t max_items = 0;
+  uint64_t max_total_bytes = 0;
+  uint32_t ratio_pct = 210;
+  uint64_t pool_bytes = 0;
+  uint64_t group_flags_n = 0, block_flags_n = 0;
+  uint8_t* base = nullptr;
+  uint64_t bytes = 0;
+  BatchDev dev{};
+  uint8_t* pool = nullptr;
+  // pinned descriptor buffers: a ring for eager calls, and one buffer per
+  // captured call (a captured copy re-reads its source at every replay)
+  BatchItem* staging[kStagingRing + kCaptureSlots] = {};
+  cudaEvent_t staged[kStagingRing] = {};
+  int next = 0, next_capture = 0;
+  LaunchCfg lcfg;
+  BatchCfg cfg;
+  uint32_t last_count = 0;
+};
+
+namespace {
+
+// Lay out one call's buffers: fills `h` (count descriptors) and the totals.
+mans_status layout(mans_batch* b, const mans_batch_item* items, uint32_t count, bool compress,
+                   BatchItem* h, uint64_t* total_groups, uint64_t* max_units) {
+  uint64_t off = 0, groups = 0, units = 0, total = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const mans_batch_item& it = items[i];
+    const uint64_t eb = elem_bytes((uint32_t)it.dtype);
+    if (eb == 0) return MANS_ERR_INVALID_ARG;
+    const uint64_t bytes = it.n_elems * eb;
+    if ((!it.d_in && (bytes || !compress)) || (!it.d_out && (bytes || compress)))
+      return MANS_ERR_INVALID_ARG;
+    if ((it.d_in && !aligned16(it.d_in)) || (it.d_out && !aligned16(it.d_out)))
+      return MANS_ERR_ALIGNMENT;
+    if (compress && (it.precision < 9 || it.precision > 11)) return MANS_ERR_UNSUPPORTED_PRECISION;
+    total += bytes;
+    BatchItem& d = h[i];
+    d.in = static_cast<const uint8_t*>(it.d_in);
+    d.out = static_cast<uint8_t*>(it.d_out);
+    d.out_size = reinterpret_cast<unsigned long long*>(it.d_out_size);
+    d.n = it.n_elems;
+    d.in_bytes = it.in_bytes;
+    d.out_cap = it.out_capacity;
+    d.dtype = (uint32_t)it.dtype;
+    d.prob_bits = compress ? (uint32_t)it.precision : 0u;
+    d.group_base = groups;
+    if (it.dtype == MANS_U8) {
+      if (bytes > kMaxMerged) return MANS_ERR_TOO_LARGE;
+      d.m = nullptr;
+      d.m_cap = 0;
+      // compress: histogram chunks; decompress: no inverse mapping
+      if (compress) groups += div_up_u64(bytes, 4096);
+      units += div_up_u64(bytes, kAnsBlock);
+    } else {
+      const uint64_t g = div_up_u64(it.n_elems, kAdmGroup);
+      const uint64_t hdr = it.dtype == MANS_U16 ? 6 * g : 40 * g;
+      const uint64_t cap = std::min(mapped_cap(bytes, b->ratio_pct), kMaxMerged);
+      d.m = b->pool + off + merged_pad(hdr);
+      d.m_cap = cap;
+      off += align_up(cap + kItemSlack, 256);
+      groups += g;
+      units += div_up_u64(cap, kAnsBlock);
+    }
+  }
+  if (total > b->max_total_bytes || off > b->pool_bytes || groups > b->group_flags_n ||
+      units > b->block_flags_n)
+    return MANS_ERR_TOO_LARGE;
+  *total_groups = groups;
+  *max_units = units;
+  return MANS_OK;
+}
+
+mans_status upload(mans_batch* b, const BatchItem* h, uint32_t count, cudaStream_t s) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return MANS_ERR_CUDA;
+  BatchItem* stage;
+  if (cap == cudaStreamCaptureStatusActive) {
+    // A captured copy re-reads its source at every replay: each capture
+    // takes the next of the capture buffers, so the graphs of the last
+    // kCaptureSlots captures stay valid.
+    stage = b->staging[kStagingRing + b->next_capture];
+    b->next_capture = (b->next_capture + 1) % kCaptureSlots;
+    memcpy(stage, h, sizeof(BatchItem) * count);
+    if (cudaMemcpyAsync(b->dev.items, stage, sizeof(BatchItem) * count, cudaMemcpyHostToDevice,
+                        s) != cudaSuccess)
+      return MANS_ERR_CUDA;
+    return MANS_OK;
+  }
+  const int k = b->next;
+  b->next = (k + 1) % kStagingRing;
+  // the copy issued from this staging buffer two calls ago has finished
+  if (cudaEventSynchronize(b->staged[k]) != cudaSuccess) return MANS_ERR_CUDA;
+  stage = b->staging[k];
+  memcpy(stage, h, sizeof(BatchItem) * count);
+  if (cudaMemcpyAsync(b->dev.items, stage, sizeof(BatchItem) * count, cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    return MANS_ERR_CUDA;
+  if (cudaEventRecord(b->staged[k], s) != cudaSuccess) return MANS_ERR_CUDA;
+  return MANS_OK;
+}
+
+mans_status run(mans_batch* b, const mans_batch_item* items, uint32_t count, bool compress,
+                cudaStream_t s) {
+  if (!b || (!items && count)) return MANS_ERR_INVALID_ARG;
+  if (count > b->max_items) return MANS_ERR_TOO_LARGE;
+  if (count == 0) return MANS_OK;
+  std::vector<BatchItem> h(count);
+  uint64_t groups = 0, units = 0;
+  mans_status st = layout(b, items, count, compress, h.data(), &groups, &units);
+  if (st != MANS_OK) return st;
+  st = upload(b, h.data(), count, s);
+  if (st != MANS_OK) return st;
+  b->last_count = count;
+  cudaError_t e = compress ? launch_batch_compress(b->dev, count, groups, units, b->cfg, s)
+                           : launch_batch_decompress(b->dev, count, groups,
+                                                     div_up_u64(units, 8), b->cfg, s);
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+// Order-independent fold of every buffer's status and stream bytes (device),
+// used by the tuner to check that a schedule changes no byte.
+__global__ void batch_checksum_kernel(const BatchItem* items, const BatchState* states,
+                                      uint32_t count, unsigned long long* out) {
+  unsigned long long h = 0;
+  for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
+    const BatchItem& it = items[i];
+    if (threadIdx.x == 0) h += (unsigned long long)states[i].status * 0xD6E8FEB86659FD93ull;
+    const unsigned long long sz = it.out_size ? *it.out_size : 0ull;
+    for (unsigned long long k = threadIdx.x; k < sz; k += blockDim.x)
+      h += ((unsigned long long)it.out[k] + 1ull) * (0x9E3779B97F4A7C15ull ^ (k * 0x100000001B3ull)) *
+           (i + 1);
+  }
+  atomicAdd(out, h);
+}
+
+}  // namespace
+
+extern "C" {
+
+mans_status mans_batch_create(mans_batch** out, uint32_t max_items, uint64_t max_total_bytes,
+                              uint32_t merged_ratio_pct) {
+  if (!out || max_items == 0) return MANS_ERR_INVALID_ARG;
+  if (merged_ratio_pct == 0) merged_ratio_pct = 210;
+  if (merged_ratio_pct < 50 || merged_ratio_pct > 10000) return MANS_ERR_INVALID_ARG;
+  *out = nullptr;
+  auto* b = new (std::nothrow) mans_batch();
+  if (!b) return MANS_ERR_OUT_OF_MEMORY;
+  if (cudaGetDevice(&b->device) != cudaSuccess) {
+    delete b;
+    return MANS_ERR_CUDA;
+  }
+  init_launch_cfg(b->lcfg, b->device);
+  init_batch_cfg(b->cfg, b->lcfg);
+  b->max_items = max_items;
+  b->max_total_bytes = max_total_bytes;
+  b->ratio_pct = merged_ratio_pct;
+  b->pool_bytes = mapped_cap(max_total_bytes, merged_ratio_pct) + (uint64_t)max_items * (kItemSlack + 256 + 4096);
+  b->group_flags_n = max_total_bytes / 1024 + max_items + 2;
+  b->block_flags_n = b->pool_bytes / kAnsBlock + max_total_bytes / kAnsBlock + max_items + 2;
+  const uint64_t o_ctrl = 0;
+  const uint64_t o_items = align_up(sizeof(Ctrl), 256);
+  const uint64_t o_states = align_up(o_items + sizeof(BatchItem) * (uint64_t)max_items, 256);
+  const uint64_t o_iflags = align_up(o_states + sizeof(BatchState) * (uint64_t)max_items, 256);
+  const uint64_t o_gflags = align_up(o_iflags + 8ull * max_items, 256);
+  const uint64_t o_bflags = align_up(o_gflags + 8 * b->group_flags_n, 256);
+  const uint64_t o_slots = align_up(o_bflags + 8 * b->block_flags_n, 256);
+  const uint64_t o_pool = align_up(o_slots + batch_slot_bytes(b->cfg), 256);
+  b->bytes = align_up(o_pool + b->pool_bytes, 256);
+  if (cudaMalloc(&b->base, b->bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete b;
+    return MANS_ERR_OUT_OF_MEMORY;
+  }
+  if (cudaMemset(b->base, 0, o_slots) != cudaSuccess) {
+    cudaFree(b->base);
+    delete b;
+    return MANS_ERR_CUDA;
+  }
+  b->dev.ctrl = reinterpret_cast<Ctrl*>(b->base + o_ctrl);
+  b->dev.items = reinterpret_cast<BatchItem*>(b->base + o_items);
+  b->dev.states = reinterpret_cast<BatchState*>(b->base + o_states);
+  b->dev.item_flags = reinterpret_cast<unsigned long long*>(b->base + o_iflags);
+  b->dev.group_flags = reinterpret_cast<unsigned long long*>(b->base + o_gflags);
+  b->dev.block_flags = reinterpret_cast<unsigned long long*>(b->base + o_bflags);
+  b->dev.slots = b->base + o_slots;
+  b->pool = b->base + o_pool;
+  for (int k = 0; k < kStagingRing + kCaptureSlots; ++k) {
+    if (cudaMallocHost(&b->staging[k], sizeof(BatchItem) * (uint64_t)max_items) != cudaSuccess) {
+      mans_batch_destroy(b);
+      return MANS_ERR_OUT_OF_MEMORY;
+    }
+  }
+  for (int k = 0; k < kStagingRing; ++k) {
+    if (cudaEventCreateWithFlags(&b->staged[k], cudaEventDisableTiming) != cudaSuccess) {
+      mans_batch_destroy(b);
+      return MANS_ERR_CUDA;
+    }
+  }
+  *out = b;
+  return MANS_OK;
+}
+
+mans_status mans_batch_destroy(mans_batch* b) {
+  if (!b) return MANS_ERR_INVALID_ARG;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  for (auto& e : b->staged)
+    if (e) cudaEventDestroy(e);
+  for (auto& p : b->staging)
+    if (p) cudaFreeHost(p);
+  cudaError_t e = b->base ? cudaFree(b->base) : cudaSuccess;
+  cudaSetDevice(prev);
+  delete b;
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+uint64_t mans_batch_device_bytes(const mans_batch* b) { return b ? b->bytes : 0; }
+
+mans_status mans_batch_compress(mans_batch* b, const mans_batch_item* items, uint32_t count,
+                                mans_stream_t stream) {
+  return run(b, items, count, true, reinterpret_cast<cudaStream_t>(stream));
+}
+
+mans_status mans_batch_decompress(mans_batch* b, const mans_batch_item* items, uint32_t count,
+                                  mans_stream_t stream) {
+  return run(b, items, count, false, reinterpret_cast<cudaStream_t>(stream));
+}
+
+mans_status mans_batch_status(mans_batch* b, mans_stream_t stream, uint32_t* item_status,
+                              uint64_t* item_detail, uint32_t count) {
+  if (!b) return MANS_ERR_INVALID_ARG;
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  uint32_t first = 0;
+  if (cudaMemcpy(&first, &b->dev.ctrl->status, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  const uint32_t n = std::min(count, b->max_items);
+  if (n && (item_status || item_detail)) {
+    std::vector<BatchState> tmp(n);
+    if (cudaMemcpy(tmp.data(), b->dev.states, sizeof(BatchState) * n, cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+      return MANS_ERR_CUDA;
+    for (uint32_t i = 0; i < n; ++i) {
+      if (item_status) item_status[i] = tmp[i].status;
+      if (item_detail) item_detail[i] = tmp[i].detail;
+    }
+  }
+  return (mans_status)first;
+}
+
+mans_status mans_batch_get_schedule(const mans_batch* b, int ctas_per_sm[6], int max_ctas_per_sm[6]) {
+  if (!b) return MANS_ERR_INVALID_ARG;
+  for (int s = 0; s < kStages; ++s) {
+    if (ctas_per_sm) ctas_per_sm[s] = b->cfg.ctas_per_sm[s];
+    if (max_ctas_per_sm) max_ctas_per_sm[s] = b->cfg.occ[s];
+  }
+  return MANS_OK;
+}
+
+mans_status mans_batch_set_schedule(mans_batch* b, const int ctas_per_sm[6]) {
+  if (!b || !ctas_per_sm) return MANS_ERR_INVALID_ARG;
+  for (int s = 0; s < kStages; ++s)
+    if (ctas_per_sm[s] < 1 || ctas_per_sm[s] > b->cfg.occ[s]) return MANS_ERR_INVALID_ARG;
+  for (int s = 0; s < kStages; ++s) b->cfg.ctas_per_sm[s] = ctas_per_sm[s];
+  return MANS_OK;
+}
+
+mans_status mans_batch_autotune(mans_batch* b, const mans_batch_item* items, uint32_t count,
+                                mans_stream_t stream, float* best_ms) {
+  if (!b) return MANS_ERR_INVALID_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  unsigned long long* d_sum = nullptr;
+  if (cudaMalloc(&d_sum, sizeof(unsigned long long)) != cudaSuccess) return MANS_ERR_OUT_OF_MEMORY;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const BatchCfg start = b->cfg;
+  BatchCfg best = start;
+  float best_t = 1e30f;
+  unsigned long long ref_sum = 0;
+  bool have_ref = false;
+  mans_status st = MANS_OK;
+  // candidate resident CTAs per SM for the two heavy compress stages
+  std::vector<int> cm, ce;
+  for (int v = start.occ[kStageMap]; v >= 1; v = v > 2 ? v / 2 : v - 1) cm.push_back(v);
+  for (int v = start.occ[kStageEncode]; v >= 1; v = v > 2 ? v / 2 : v - 1) ce.push_back(v);
+  for (int m : cm) {
+    for (int en : ce) {
+      b->cfg = start;
+      b->cfg.ctas_per_sm[kStageMap] = m;
+      b->cfg.ctas_per_sm[kStageEncode] = en;
+      float tm = 0;
+      for (int rep = 0; rep < 2 && st == MANS_OK; ++rep) {  // first run warms up
+        cudaEventRecord(e0, s);
+        st = mans_batch_compress(b, items, count, stream);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = MANS_ERR_CUDA;
+        cudaEventElapsedTime(&tm, e0, e1);
+      }
+      if (st != MANS_OK) break;
+      cudaMemsetAsync(d_sum, 0, sizeof(unsigned long long), s);
+      batch_checksum_kernel<<<b->cfg.sms, 256, 0, s>>>(b->dev.items, b->dev.states, count, d_sum);
+      unsigned long long sum = 0;
+      cudaMemcpyAsync(&sum, d_sum, sizeof(sum), cudaMemcpyDeviceToHost, s);
+      cudaStreamSynchronize(s);
+      if (!have_ref) {
+        ref_sum = sum;
+        have_ref = true;
+      } else if (sum != ref_sum) {
+        continue;  // a schedule that changed the bytes is never chosen
+      }
+      if (tm < best_t) {
+        best_t = tm;
+        best = b->cfg;
+      }
+    }
+    if (st != MANS_OK) break;
+  }
+  b->cfg = st == MANS_OK ? best : start;
+  // leave the outputs of the chosen schedule in place
+  if (st == MANS_OK) st = mans_batch_compress(b, items, count, stream);
+  if (st == MANS_OK && cudaStreamSynchronize(s) != cudaSuccess) st = MANS_ERR_CUDA;
+  if (best_ms) *best_ms = best_t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_sum);
+  return st;
+}
+
+}  // extern "C"

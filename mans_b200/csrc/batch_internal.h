@@ -1,0 +1,77 @@
+// batch_internal.h -- device descriptors and launch interface of the batched
+// codec (batch.cu). Not part of the public API.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mans_internal.h"
+
+namespace mans {
+
+struct Ctrl;
+
+// One buffer of a batch, built by the host for every call.
+struct BatchItem {
+  const uint8_t* in;             // compress: values; decompress: stream
+  uint8_t* out;                  // compress: stream; decompress: values
+  unsigned long long* out_size;  // compress: stream bytes (device, may be null)
+  uint64_t n;                    // elements
+  uint64_t in_bytes;             // decompress: stream bytes available
+  uint64_t out_cap;              // compress: stream capacity
+  uint8_t* m;                    // mapped bytes (per-element section 16-byte aligned)
+  uint64_t m_cap;
+  uint64_t group_base;           // first global mapping unit of this buffer
+  uint32_t dtype;                // MANS_U8 / MANS_U16 / MANS_U32
+  uint32_t prob_bits;
+};
+
+// Per-buffer device state (kept in the batch workspace).
+struct BatchState {
+  uint32_t hist[256];
+  uint2 enc[256];
+  uint32_t pdf[256];
+  unsigned long long msize;   // mapped bytes (compress) / decoded bytes (decompress)
+  unsigned long long detail;  // detail of the buffer's first error
+  uint32_t status;            // the buffer's first error (mans_status)
+  uint32_t nb;                // rANS blocks
+  uint32_t unit_base;         // first global block (compress) / decode chunk (decompress)
+  uint32_t n_hdr, cw, p;      // decompress: header fields
+};
+
+struct BatchDev {
+  Ctrl* ctrl;
+  BatchItem* items;
+  BatchState* states;
+  unsigned long long* item_flags;
+  unsigned long long* group_flags;
+  unsigned long long* block_flags;
+  uint8_t* slots;
+};
+
+enum BatchStage {
+  kStageMap = 0,
+  kStagePlanEnc,
+  kStageEncode,
+  kStagePlanDec,
+  kStageDecode,
+  kStageUnmap,
+  kStages
+};
+
+// Schedule of the batched kernels: resident CTAs per SM of each stage
+// (ctas_per_sm <= occ). The bytes produced do not depend on it.
+struct BatchCfg {
+  int sms = 148;
+  int occ[kStages] = {1, 1, 1, 1, 1, 1};
+  int ctas_per_sm[kStages] = {1, 1, 1, 1, 1, 1};
+};
+
+void init_batch_cfg(BatchCfg& c, const LaunchCfg& base);
+uint64_t batch_slot_bytes(const BatchCfg& c);
+cudaError_t launch_batch_compress(const BatchDev& d, uint32_t count, uint64_t total_groups,
+                                  uint64_t max_blocks, const BatchCfg& c, cudaStream_t s);
+cudaError_t launch_batch_decompress(const BatchDev& d, uint32_t count, uint64_t total_groups,
+                                    uint64_t max_chunks, const BatchCfg& c, cudaStream_t s);
+
+}  // namespace mans

@@ -41,7 +41,6 @@ struct mans_workspace {
   uint64_t ans_flags_n = 0;
   uint8_t* merged = nullptr;  // 16-byte aligned region of merged_cap + slack bytes
   uint8_t* enc_slots = nullptr;  // per-warp word slots of the encode kernel
-  uint32_t epoch = 0;
   LaunchCfg cfg;
   // Opt-in kernel timing: a ring of event triples per recorded call
   // (compress: start, after mapping, after encode; decompress: start, after
@@ -83,12 +82,6 @@ constexpr uint64_t kSlack = 256;
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
-
-uint32_t next_epoch(mans_workspace* ws) {
-  ws->epoch = (ws->epoch + 1) & 0x3fffffffu;
-  if (ws->epoch == 0) ws->epoch = 1;
-  return ws->epoch;
-}
 
 uint64_t elem_bytes(mans_dtype d) {
   switch (d) {
@@ -216,7 +209,6 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
   if (in_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   unsigned long long* osz = reinterpret_cast<unsigned long long*>(d_out_size);
-  const uint32_t epoch = next_epoch(ws);
   cudaError_t e = cudaSuccess;
   if (dtype == MANS_U8 && in_bytes > kMaxMerged) return MANS_ERR_TOO_LARGE;
   mark(ws, 0, s);
@@ -225,7 +217,7 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
     mark(ws, 1, s);
     if (e == cudaSuccess)
       e = launch_ans_encode((const uint8_t*)d_in, (uint8_t*)d_out, out_capacity, osz, nullptr,
-                            ws->ctrl, ws->ans_flags, epoch, precision,
+                            ws->ctrl, ws->ans_flags, precision,
                             div_up_u64(in_bytes, kAnsBlock), ws->cfg, s, ws->enc_slots);
   } else if (dtype == MANS_U16) {
     const uint64_t hdr = adm_u16_header_bytes(n_elems);
@@ -233,22 +225,22 @@ mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in
     if (hdr + n_elems + 32 * g > ws->merged_cap) return MANS_ERR_TOO_LARGE;
     uint8_t* m = ws->merged + merged_pad(hdr);
     e = launch_adm_u16_map((const uint16_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
-                           ws->adm_flags, epoch, precision, ws->cfg, s);
+                           ws->adm_flags, precision, ws->cfg, s);
     mark(ws, 1, s);
     if (e == cudaSuccess)
       e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
-                            ws->ans_flags, epoch, precision,
+                            ws->ans_flags, precision,
                             div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s, ws->enc_slots);
   } else {
     const uint64_t hdr = adm_u32_header_bytes(n_elems);
     if (hdr + n_elems > ws->merged_cap) return MANS_ERR_TOO_LARGE;
     uint8_t* m = ws->merged + merged_pad(hdr);
     e = launch_adm_u32_map((const uint32_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
-                           ws->adm_flags, epoch, precision, ws->cfg, s);
+                           ws->adm_flags, precision, ws->cfg, s);
     mark(ws, 1, s);
     if (e == cudaSuccess)
       e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
-                            ws->ans_flags, epoch, precision,
+                            ws->ans_flags, precision,
                             div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s, ws->enc_slots);
   }
   mark(ws, 2, s);
@@ -393,11 +385,10 @@ mans_status mans_ans_encode(int precision, const uint8_t* d_in, uint32_t in_size
   mans_status st = MANS_OK;
   mans_workspace* ws = default_ws(s, in_size, &st);
   if (!ws) return st;
-  const uint32_t epoch = next_epoch(ws);
   cudaError_t e = launch_hist_bytes(d_in, in_size, ws->ctrl, precision, ws->cfg, s);
   if (e == cudaSuccess)
     e = launch_ans_encode(d_in, d_out, ans_bound(in_size), nullptr, d_out_size, ws->ctrl,
-                          ws->ans_flags, epoch, precision, div_up_u64(in_size, kAnsBlock),
+                          ws->ans_flags, precision, div_up_u64(in_size, kAnsBlock),
                           ws->cfg, s, ws->enc_slots);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
 }

@@ -47,11 +47,33 @@ struct Ctrl {
   uint32_t pdf[kAnsSyms];
   unsigned long long merged_size;  // merged bytes of the current call
   uint32_t total_words;
-  uint32_t pad1;
+  // Look-back epoch of the current call: read by every kernel of a compress,
+  // advanced by the last CTA of its final kernel, so a call needs no host
+  // bookkeeping and a captured CUDA graph stays correct across replays.
+  uint32_t epoch;
 };
 
 __device__ __forceinline__ void report_error(Ctrl* c, uint32_t code, unsigned long long detail) {
   if (atomicCAS(&c->status, 0u, code) == 0u) c->detail = detail;
+}
+
+// Where device-side errors of one unit of work go: the call's control block
+// and, in a batch, the buffer's own status (first error wins in each).
+struct Sink {
+  uint32_t* status;
+  unsigned long long* detail;
+  uint32_t* item_status;
+  unsigned long long* item_detail;
+};
+__device__ __forceinline__ Sink sink_of(Ctrl* c) {
+  return Sink{&c->status, &c->detail, nullptr, nullptr};
+}
+__device__ __forceinline__ void report(const Sink& s, uint32_t code, unsigned long long detail) {
+  if (atomicCAS(s.status, 0u, code) == 0u) *s.detail = detail;
+  if (s.item_status && atomicCAS(s.item_status, 0u, code) == 0u) *s.item_detail = detail;
+}
+__device__ __forceinline__ bool sink_failed(const Sink& s) {
+  return *((volatile uint32_t*)s.status) != 0;
 }
 
 __device__ __forceinline__ int lane_id() {
@@ -155,7 +177,7 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 // returns the same value. On timeout reports MANS_ERR_TIMEOUT and returns the
 // partial sum (the call's output is then invalid, but the kernel finishes).
 __device__ __forceinline__ uint32_t lookback_exclusive(unsigned long long* flags, uint32_t tile,
-                                                       uint32_t epoch, Ctrl* ctrl) {
+                                                       uint32_t epoch, const Sink& sink) {
   const int lane = lane_id();
   uint32_t excl = 0;
   int64_t base = (int64_t)tile - 1;
@@ -175,8 +197,8 @@ __device__ __forceinline__ uint32_t lookback_exclusive(unsigned long long* flags
         // Give up after the bound, or at once when another waiter already
         // recorded an error (so one expired wait does not multiply).
         if (spins > kSpinLimit ||
-            ((spins & 63u) == 0 && *((volatile uint32_t*)&ctrl->status) == MANS_ERR_TIMEOUT)) {
-          report_error(ctrl, MANS_ERR_TIMEOUT, tile);
+            ((spins & 63u) == 0 && *((volatile uint32_t*)sink.status) == MANS_ERR_TIMEOUT)) {
+          report(sink, MANS_ERR_TIMEOUT, tile);
           st = kFlagIncl;
           w = 0;
           break;
@@ -197,6 +219,12 @@ __device__ __forceinline__ uint32_t lookback_exclusive(unsigned long long* flags
     base -= kWarp;
   }
   return excl;
+}
+
+__device__ __forceinline__ uint32_t warp_claim(uint32_t* counter, int lane) {
+  uint32_t v = 0;
+  if (lane == 0) v = atomicAdd(counter, 1u);
+  return __shfl_sync(0xffffffffu, v, 0);
 }
 
 __host__ __device__ inline uint64_t div_up_u64(uint64_t a, uint64_t b) { return (a + b - 1) / b; }

@@ -31,9 +31,8 @@ cudaError_t launch_hist_bytes(const uint8_t* in, uint64_t n, Ctrl* ctrl, int pro
 // blocks in flight, or nullptr to compact them in shared memory instead.
 cudaError_t launch_ans_encode(const uint8_t* in, uint8_t* out, uint64_t out_cap,
                               unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
-                              unsigned long long* flags, uint32_t epoch, int prob_bits,
-                              uint64_t max_blocks, const LaunchCfg& cfg, cudaStream_t s,
-                              uint8_t* slots);
+                              unsigned long long* flags, int prob_bits, uint64_t max_blocks,
+                              const LaunchCfg& cfg, cudaStream_t s, uint8_t* slots);
 uint64_t ans_encode_slot_bytes(const LaunchCfg& cfg);
 // Decode the stream at `in` into `out` (at most out_cap bytes). expect_p < 0
 // accepts any valid precision. record != 0 stores the decoded size in ctrl.
@@ -45,15 +44,15 @@ cudaError_t launch_ans_decode(const uint8_t* in, uint64_t in_size, uint8_t* out,
 // Map n values into the merged buffer M (16-byte aligned codes section),
 // histogram it and normalise (ctrl). flags: >= ceil(n/4096) entries.
 cudaError_t launch_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* m, uint64_t m_cap,
-                               Ctrl* ctrl, unsigned long long* flags, uint32_t epoch,
-                               int prob_bits, const LaunchCfg& cfg, cudaStream_t s);
+                               Ctrl* ctrl, unsigned long long* flags, int prob_bits,
+                               const LaunchCfg& cfg, cudaStream_t s);
 cudaError_t launch_adm_u16_unmap(const uint8_t* m, uint64_t n, uint16_t* out, Ctrl* ctrl,
                                  const LaunchCfg& cfg, cudaStream_t s);
 
 // ---- ADM uint32 (adm_u32.cu) ----
 cudaError_t launch_adm_u32_map(const uint32_t* in, uint64_t n, uint8_t* m, uint64_t m_cap,
-                               Ctrl* ctrl, unsigned long long* flags, uint32_t epoch,
-                               int prob_bits, const LaunchCfg& cfg, cudaStream_t s);
+                               Ctrl* ctrl, unsigned long long* flags, int prob_bits,
+                               const LaunchCfg& cfg, cudaStream_t s);
 cudaError_t launch_adm_u32_unmap(const uint8_t* m, uint64_t n, uint32_t* out, Ctrl* ctrl,
                                  const LaunchCfg& cfg, cudaStream_t s);
 
