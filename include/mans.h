@@ -183,6 +183,14 @@ mans_status mans_batch_decompress(mans_batch* b, const mans_batch_item* items, u
  * the first `count` buffers' statuses and details (either may be NULL). */
 mans_status mans_batch_status(mans_batch* b, mans_stream_t stream, uint32_t* item_status,
                               uint64_t* item_detail, uint32_t count);
+/* Opt-in stage timing: when enabled, CUDA events are recorded around the
+ * stages of up to 64 compress and 64 decompress calls that are not being
+ * captured (no synchronisation is added). */
+mans_status mans_batch_set_timing(mans_batch* b, int enable);
+/* Summed milliseconds of the recorded calls' stages (ms[0..2] compress: map
+ * with histogram, plan, encode; ms[3..5] decompress: plan, decode, unmap) and
+ * the numbers of recorded calls; waits for the events, then clears them. */
+mans_status mans_batch_stage_times(mans_batch* b, float ms[6], int calls[2]);
 /* Schedule: resident CTAs per SM of each stage (map, plan, encode,
  * decode plan, decode, unmap); never changes the bytes produced. */
 mans_status mans_batch_get_schedule(const mans_batch* b, int ctas_per_sm[6],

@@ -60,6 +60,8 @@ SIGNATURES = {
     "mans_batch_compress": (_i32, [_vp, _vp, _u32, _vp]),
     "mans_batch_decompress": (_i32, [_vp, _vp, _u32, _vp]),
     "mans_batch_status": (_i32, [_vp, _vp, C.POINTER(_u32), C.POINTER(_u64), _u32]),
+    "mans_batch_set_timing": (_i32, [_vp, _i32]),
+    "mans_batch_stage_times": (_i32, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "mans_batch_get_schedule": (_i32, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "mans_batch_set_schedule": (_i32, [_vp, C.POINTER(C.c_int)]),
     "mans_batch_autotune": (_i32, [_vp, _vp, _u32, _vp, C.POINTER(C.c_float)]),

@@ -89,6 +89,18 @@ class Batch:
             bad = [i for i, v in enumerate(st) if v]
             raise MansError(first, f"{what}: buffers {bad[:8]} (detail {det[bad[0]] if bad else 0})")
 
+    def set_timing(self, enable: bool = True) -> None:
+        _check(load().mans_batch_set_timing(self.h, int(enable)), "mans_batch_set_timing")
+
+    def stage_times(self) -> dict:
+        """Summed stage milliseconds and call counts recorded since the last read."""
+        ms = (C.c_float * 6)()
+        calls = (C.c_int * 2)()
+        _check(load().mans_batch_stage_times(self.h, ms, calls), "mans_batch_stage_times")
+        d = {name: ms[i] for i, name in enumerate(STAGES)}
+        d["compress_calls"], d["decompress_calls"] = calls[0], calls[1]
+        return d
+
     def schedule(self) -> tuple[list[int], list[int]]:
         cur = (C.c_int * 6)()
         mx = (C.c_int * 6)()

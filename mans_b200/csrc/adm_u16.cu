@@ -34,7 +34,7 @@ __global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
   hist_merge_and_normalize(s_h, kMapWarps, ctrl, g == 0 ? 0ull : ~0ull, 0, prob_bits);
 }
 
-__global__ __launch_bounds__(kUnmapThreads) void adm_u16_unmap_kernel(
+__global__ __launch_bounds__(kUnmapThreads, 4) void adm_u16_unmap_kernel(
     const uint8_t* __restrict__ M, uint64_t n, uint16_t* __restrict__ out, Ctrl* ctrl) {
   const Sink sink = sink_of(ctrl);
   if (sink_failed(sink)) return;

@@ -55,62 +55,181 @@ __global__ void batch_begin_kernel(BatchState* states, uint32_t count, Ctrl* ctr
 }
 
 // ------------------------------------------------------------------------
-// Compress stage 1: mapping over the global group space.
+// Compress stage 1: mapping, one launch per dtype over that dtype's unit
+// space (units of other dtypes' buffers are empty), so each launch carries
+// only its own code path, registers and shared memory. As in the
+// single-buffer mappers, units are claimed one at a time and the unit one
+// grid of warps ahead is prefetched into L2 (a second forward cursor finds
+// its buffer).
 // ------------------------------------------------------------------------
 struct BatchMapSmem {
   alignas(16) uint8_t stage[kBWarps][kGroupRecMax + 16];
 };
 
-__device__ __forceinline__ void flush_hist(uint32_t* h, uint32_t* dst, int lane) {
-  __syncwarp();
-  for (int i = lane; i < kAnsSyms; i += 32) {
-    const uint32_t v = h[i];
-    if (v) {
-      atomicAdd(&dst[i], v);
-      h[i] = 0;
+// Histogram merging. Every warp counts into its own shared histogram. When
+// it leaves a buffer, it adds those counts into a CTA-level slot for that
+// buffer (shared by the CTA's warps on the same buffer, reference counted);
+// the last warp to leave a slot adds it into the buffer's global histogram.
+// So a buffer that the whole GPU works on at once is merged into global
+// memory about once per CTA instead of once per warp. A warp that finds its
+// slot taken by another buffer merges straight into global memory.
+constexpr int kCtaSlots = 4;
+struct MapHist {
+  uint32_t warp[kBWarps][kAnsSyms];
+  uint32_t slot[kCtaSlots][kAnsSyms];
+  uint32_t state[kCtaSlots];  // 0 free; else (buffer + 1) << 12 | warps inside
+};
+
+__device__ __forceinline__ uint32_t* item_hist(uint32_t* hists, uint32_t hist_items, uint32_t item) {
+  return hists + ((uint64_t)(blockIdx.x % kHistCopies) * hist_items + item) * kAnsSyms;
+}
+
+// Enter buffer `item`: the slot index, or -1 when its slot is busy.
+__device__ __forceinline__ int hist_enter(MapHist& mh, uint32_t item, int lane) {
+  int k = -1;
+  if (lane == 0) {
+    const int s = (int)(item % kCtaSlots);
+    const uint32_t tag = (item + 1) << 12;
+    uint32_t old = *((volatile uint32_t*)&mh.state[s]);
+    for (int tries = 0; tries < 8; ++tries) {
+      uint32_t nv;
+      if (old == 0) nv = tag | 1u;
+      else if ((old & ~0xfffu) == tag && (old & 0xfffu) != 0) nv = old + 1;
+      else break;  // another buffer, or this one being merged out
+      const uint32_t prev = atomicCAS(&mh.state[s], old, nv);
+      if (prev == old) {
+        k = s;
+        break;
+      }
+      old = prev;
     }
+  }
+  return __shfl_sync(0xffffffffu, k, 0);
+}
+
+__device__ __forceinline__ void hist_leave(MapHist& mh, int slot, uint32_t* wh, uint32_t* gh,
+                                           int lane) {
+  __syncwarp();
+  if (slot < 0) {
+    for (int i = lane; i < kAnsSyms; i += 32) {
+      const uint32_t v = wh[i];
+      if (v) {
+        atomicAdd(&gh[i], v);
+        wh[i] = 0;
+      }
+    }
+    __syncwarp();
+    return;
+  }
+  uint32_t* sh = mh.slot[slot];
+  for (int i = lane; i < kAnsSyms; i += 32) {
+    const uint32_t v = wh[i];
+    if (v) {
+      atomicAdd(&sh[i], v);
+      wh[i] = 0;
+    }
+  }
+  __threadfence_block();
+  __syncwarp();
+  uint32_t last = 0;
+  if (lane == 0) last = (atomicSub(&mh.state[slot], 1u) & 0xfffu) == 1u;
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (last) {
+    // no warp can add to the slot now (entering needs a nonzero count)
+    __threadfence_block();
+    for (int i = lane; i < kAnsSyms; i += 32) {
+      const uint32_t v = sh[i];
+      if (v) {
+        atomicAdd(&gh[i], v);
+        sh[i] = 0;
+      }
+    }
+    __threadfence_block();
+    __syncwarp();
+    if (lane == 0) atomicExch(&mh.state[slot], 0u);
   }
   __syncwarp();
 }
 
-__global__ __launch_bounds__(kBThreads) void batch_map_kernel(const BatchItem* __restrict__ items,
+// Bytes of unit u of a buffer of this dtype (for the L2 prefetch).
+template <uint32_t kDtype>
+__device__ __forceinline__ void unit_span(const BatchItem& b, uint64_t u, const uint8_t*& p,
+                                          uint32_t& bytes) {
+  constexpr uint32_t eb = kDtype == MANS_U8 ? 1 : kDtype == MANS_U16 ? 2 : 4;
+  constexpr uint32_t per = kDtype == MANS_U8 ? kRawChunk : kAdmGroup;
+  const uint64_t s0 = u * per;
+  p = b.in + s0 * eb;
+  bytes = (uint32_t)(min_u64(per, b.n - s0) * eb);
+}
+
+template <uint32_t kDtype>
+__global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 4) void batch_map_kernel(const BatchItem* __restrict__ items,
                                                               BatchState* states, uint32_t count,
                                                               uint64_t total_units, Ctrl* ctrl,
-                                                              unsigned long long* flags) {
+                                                              unsigned long long* flags,
+                                                              uint32_t* hists, uint32_t hist_items) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  BatchMapSmem& sm = *reinterpret_cast<BatchMapSmem*>(smem_raw);
-  __shared__ uint32_t s_h[kBWarps][kAnsSyms];
+  __shared__ MapHist mh;
+  constexpr int kSlot = 3 + (kDtype == MANS_U8 ? 0 : kDtype == MANS_U16 ? 1 : 2);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  for (int i = t; i < kBWarps * kAnsSyms; i += kBThreads) (&s_h[0][0])[i] = 0;
+  for (int i = t; i < (int)(sizeof(MapHist) / 4); i += kBThreads) reinterpret_cast<uint32_t*>(&mh)[i] = 0;
   __syncthreads();
+  uint32_t* wh = mh.warp[warp];
+  int hslot = -1;
   const uint32_t epoch = *((volatile uint32_t*)&ctrl->epoch);
-  uint32_t it = 0, cur_item = 0xffffffffu;
-  auto base = [&](uint32_t i) { return items[i].group_base; };
+  const uint64_t ahead = (uint64_t)gridDim.x * kBWarps;
+  uint32_t it = 0, pit = 0, cur_item = 0xffffffffu;
+  auto base = [&](uint32_t i) {
+    const BatchItem& x = items[i];
+    return x.dtype == kDtype ? x.group_base : ~0ull;  // other dtypes: empty, skipped below
+  };
+  // Forward scan in this dtype's unit space: buffers of other dtypes hold no
+  // units, so the owner of u is the last buffer of this dtype with base <= u.
+  auto owner = [&](uint32_t from, uint64_t u) {
+    uint32_t k = from;
+    for (uint32_t j = from + 1; j < count; ++j) {
+      const uint64_t bj = base(j);
+      if (bj == ~0ull) continue;
+      if (bj > u) break;
+      k = j;
+    }
+    return k;
+  };
   while (true) {
-    const uint32_t u = warp_claim(&ctrl->tile_counter[0], lane);
+    const uint32_t u = warp_claim(&ctrl->tile_counter[kSlot], lane);
     if (u >= total_units) break;
-    it = find_item(it, count, u, base);
+    if (lane == 0 && (uint64_t)u + ahead < total_units) {
+      pit = owner(pit, (uint64_t)u + ahead);
+      const BatchItem& pb = items[pit];
+      const uint8_t* pp;
+      uint32_t pbytes;
+      unit_span<kDtype>(pb, (uint64_t)u + ahead - pb.group_base, pp, pbytes);
+      prefetch_l2(pp, pbytes);
+    }
+    it = owner(it, u);
     if (it != cur_item) {
-      if (cur_item != 0xffffffffu) flush_hist(s_h[warp], states[cur_item].hist, lane);
+      if (cur_item != 0xffffffffu)
+        hist_leave(mh, hslot, wh, item_hist(hists, hist_items, cur_item), lane);
       cur_item = it;
+      hslot = hist_enter(mh, it, lane);
     }
     const BatchItem& b = items[it];
     BatchState* st = &states[it];
     const Sink sink = item_sink(ctrl, st);
     const uint32_t grp = (uint32_t)(u - b.group_base);
-    if (b.dtype == MANS_U16) {
-      map16_group(reinterpret_cast<const uint16_t*>(b.in), b.n, b.m, b.m_cap, flags + b.group_base,
-                  &st->msize, grp, epoch, sink, s_h[warp], lane);
-    } else if (b.dtype == MANS_U32) {
-      map32_group(reinterpret_cast<const uint32_t*>(b.in), b.n, b.m, b.m_cap,
-                  flags + b.group_base, &st->msize, grp, epoch, sink, s_h[warp], sm.stage[warp],
-                  lane);
+    if constexpr (kDtype == MANS_U16) {
+      map16_group(reinterpret_cast<const uint16_t*>(b.in), b.n, b.m, b.m_cap, flags + b.flag_base,
+                  &st->msize, grp, epoch, sink, wh, lane);
+    } else if constexpr (kDtype == MANS_U32) {
+      BatchMapSmem& sm = *reinterpret_cast<BatchMapSmem*>(smem_raw);
+      map32_group(reinterpret_cast<const uint32_t*>(b.in), b.n, b.m, b.m_cap, flags + b.flag_base,
+                  &st->msize, grp, epoch, sink, wh, sm.stage[warp], lane);
     } else {
       // raw bytes: histogram one 4 KiB chunk
       const uint64_t s0 = (uint64_t)grp * kRawChunk;
       const uint32_t len = (uint32_t)min_u64(kRawChunk, b.n - s0);
       const uint8_t* p = b.in + s0;
-      uint32_t* h = s_h[warp];
+      uint32_t* h = wh;
       if (len == kRawChunk) {
         const uint4* p4 = reinterpret_cast<const uint4*>(p);
 #pragma unroll
@@ -130,18 +249,19 @@ __global__ __launch_bounds__(kBThreads) void batch_map_kernel(const BatchItem* _
       }
     }
   }
-  if (cur_item != 0xffffffffu) flush_hist(s_h[warp], states[cur_item].hist, lane);
+  if (cur_item != 0xffffffffu)
+    hist_leave(mh, hslot, wh, item_hist(hists, hist_items, cur_item), lane);
 
   __shared__ int s_last;
   __syncthreads();
   if (t == 0) {
     __threadfence();
-    s_last = atomicAdd(&ctrl->done_counter[0], 1u) == gridDim.x - 1;
+    s_last = atomicAdd(&ctrl->done_counter[kSlot], 1u) == gridDim.x - 1;
   }
   __syncthreads();
   if (s_last && t == 0) {
-    ctrl->tile_counter[0] = 0;
-    ctrl->done_counter[0] = 0;
+    ctrl->tile_counter[kSlot] = 0;
+    ctrl->done_counter[kSlot] = 0;
   }
 }
 
@@ -153,7 +273,9 @@ __global__ __launch_bounds__(kBThreads) void batch_map_kernel(const BatchItem* _
 __global__ __launch_bounds__(256) void batch_plan_encode_kernel(const BatchItem* __restrict__ items,
                                                                 BatchState* states, uint32_t count,
                                                                 Ctrl* ctrl,
-                                                                unsigned long long* item_flags) {
+                                                                unsigned long long* item_flags,
+                                                                uint32_t* hists,
+                                                                uint32_t hist_items) {
   __shared__ uint32_t s_item;
   __shared__ uint32_t s_hist[kAnsSyms];
   __shared__ int s_last;
@@ -168,10 +290,16 @@ __global__ __launch_bounds__(256) void batch_plan_encode_kernel(const BatchItem*
     BatchState* st = &states[i];
     const bool ok = *((volatile uint32_t*)&st->status) == 0;
     unsigned long long msize = b.dtype == MANS_U8 ? b.n : (b.n == 0 ? 0ull : __ldcg(&st->msize));
-    s_hist[t] = __ldcg(&st->hist[t]);
+    uint32_t hv = 0;
+#pragma unroll
+    for (int c = 0; c < kHistCopies; ++c) {
+      uint32_t* h = hists + ((uint64_t)c * hist_items + i) * kAnsSyms + t;
+      hv += __ldcg(h);
+      *h = 0;
+    }
+    s_hist[t] = hv;
     __syncthreads();
     normalize_cta(s_hist, (uint32_t)(ok ? msize : 0), (int)b.prob_bits, st->pdf, st->enc);
-    st->hist[t] = 0;
     const uint32_t nb = ok ? (uint32_t)div_up_u64(msize, kAnsBlock) : 0u;
     if (t < 32) {
       if (lane == 0) st_flag(&item_flags[i], make_flag(i == 0 ? kFlagIncl : kFlagAgg, epoch, nb));
@@ -406,25 +534,31 @@ __global__ __launch_bounds__(kBThreads) void batch_decode_kernel(const BatchItem
 }
 
 // ------------------------------------------------------------------------
-// Decompress stage 3: inverse mapping over the global group space.
+// Decompress stage 3: inverse mapping, one launch per dtype (MANS_U16,
+// MANS_U32) over that dtype's unit space.
 // ------------------------------------------------------------------------
 struct BatchUnmapSmem {
   alignas(16) uint8_t stage[kBWarps][kGroupRecMax + 48];
 };
 
+template <uint32_t kDtype>
 __global__ __launch_bounds__(kBThreads) void batch_unmap_kernel(const BatchItem* __restrict__ items,
                                                                 BatchState* states, uint32_t count,
                                                                 uint64_t total_units, Ctrl* ctrl) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  BatchUnmapSmem& sm = *reinterpret_cast<BatchUnmapSmem*>(smem_raw);
   __shared__ int s_last;
+  constexpr int kSlot = kDtype == MANS_U16 ? 2 : 6;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   uint32_t it = 0;
-  auto base = [&](uint32_t i) { return items[i].group_base; };
   while (true) {
-    const uint32_t u = warp_claim(&ctrl->tile_counter[2], lane);
+    const uint32_t u = warp_claim(&ctrl->tile_counter[kSlot], lane);
     if (u >= total_units) break;
-    it = find_item(it, count, u, base);
+    for (uint32_t j = it + 1; j < count; ++j) {
+      const BatchItem& x = items[j];
+      if (x.dtype != kDtype) continue;
+      if (x.group_base > u) break;
+      it = j;
+    }
     const BatchItem& b = items[it];
     BatchState* st = &states[it];
     if (*((volatile uint32_t*)&st->status) != 0) continue;
@@ -432,7 +566,7 @@ __global__ __launch_bounds__(kBThreads) void batch_unmap_kernel(const BatchItem*
     const uint64_t grp = u - b.group_base;
     const uint64_t g = div_up_u64(b.n, kAdmGroup);
     const uint64_t msize = st->msize;
-    if (b.dtype == MANS_U16) {
+    if constexpr (kDtype == MANS_U16) {
       const uint64_t bits_base = 6 * g + b.n;
       if (msize < bits_base || ((msize - bits_base) & 31)) {
         if (lane == 0) report(sink, MANS_ERR_CORRUPT, msize);
@@ -441,6 +575,7 @@ __global__ __launch_bounds__(kBThreads) void batch_unmap_kernel(const BatchItem*
       unmap16_group(b.m, b.n, (msize - bits_base) >> 5, reinterpret_cast<uint16_t*>(b.out), grp,
                     sink, lane);
     } else {
+      BatchUnmapSmem& sm = *reinterpret_cast<BatchUnmapSmem*>(smem_raw);
       const uint64_t rec_base = 40 * g;
       if (msize < rec_base) {
         if (lane == 0) report(sink, MANS_ERR_CORRUPT, msize);
@@ -453,12 +588,12 @@ __global__ __launch_bounds__(kBThreads) void batch_unmap_kernel(const BatchItem*
   __syncthreads();
   if (t == 0) {
     __threadfence();
-    s_last = atomicAdd(&ctrl->done_counter[2], 1u) == gridDim.x - 1;
+    s_last = atomicAdd(&ctrl->done_counter[kSlot], 1u) == gridDim.x - 1;
   }
   __syncthreads();
   if (s_last && t == 0) {
-    ctrl->tile_counter[2] = 0;
-    ctrl->done_counter[2] = 0;
+    ctrl->tile_counter[kSlot] = 0;
+    ctrl->done_counter[kSlot] = 0;
   }
 }
 
@@ -472,56 +607,92 @@ static int occ(const void* fn, int threads, size_t smem) {
 }
 
 void init_batch_cfg(BatchCfg& c, const LaunchCfg& base) {
-  cudaFuncSetAttribute(batch_map_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(batch_map_kernel<MANS_U32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(BatchMapSmem));
   cudaFuncSetAttribute(batch_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(BatchEncSmem));
   cudaFuncSetAttribute(batch_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(BatchDecSmem));
-  cudaFuncSetAttribute(batch_unmap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(batch_unmap_kernel<MANS_U32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(BatchUnmapSmem));
   c.sms = base.sms;
-  c.occ[kStageMap] = occ((const void*)batch_map_kernel, kBThreads, sizeof(BatchMapSmem));
+  // the map and unmap stages report the occupancy of their heaviest variant
+  c.occ[kStageMap] = min(occ((const void*)batch_map_kernel<MANS_U16>, kBThreads, 0),
+                         occ((const void*)batch_map_kernel<MANS_U32>, kBThreads, sizeof(BatchMapSmem)));
   c.occ[kStagePlanEnc] = occ((const void*)batch_plan_encode_kernel, 256, 0);
   c.occ[kStageEncode] = occ((const void*)batch_encode_kernel, kBThreads, sizeof(BatchEncSmem));
   c.occ[kStagePlanDec] = occ((const void*)batch_plan_decode_kernel, 32, 0);
   c.occ[kStageDecode] = occ((const void*)batch_decode_kernel, kBThreads, sizeof(BatchDecSmem));
-  c.occ[kStageUnmap] = occ((const void*)batch_unmap_kernel, kBThreads, sizeof(BatchUnmapSmem));
+  c.occ[kStageUnmap] = min(occ((const void*)batch_unmap_kernel<MANS_U16>, kBThreads, 0),
+                           occ((const void*)batch_unmap_kernel<MANS_U32>, kBThreads,
+                               sizeof(BatchUnmapSmem)));
   for (int s = 0; s < kStages; ++s) c.ctas_per_sm[s] = c.occ[s];
+  c.occ_u16_map = occ((const void*)batch_map_kernel<MANS_U16>, kBThreads, 0);
+  c.occ_u8_map = occ((const void*)batch_map_kernel<MANS_U8>, kBThreads, 0);
+  c.occ_u16_unmap = occ((const void*)batch_unmap_kernel<MANS_U16>, kBThreads, 0);
 }
 
 uint64_t batch_slot_bytes(const BatchCfg& c) {
   return (uint64_t)c.sms * c.occ[kStageEncode] * kBWarps * kEncSlotBytes;
 }
 
-static unsigned grid_of(const BatchCfg& c, int stage, uint64_t want) {
-  const uint64_t cap = (uint64_t)c.sms * (uint64_t)c.ctas_per_sm[stage];
+static unsigned grid_of(const BatchCfg& c, int stage, uint64_t want, int extra_occ = 0) {
+  // the stage's schedule, scaled for a lighter variant that fits more CTAs
+  int per_sm = c.ctas_per_sm[stage];
+  if (extra_occ > c.occ[stage]) per_sm = per_sm * extra_occ / c.occ[stage];
+  const uint64_t cap = (uint64_t)c.sms * (uint64_t)(per_sm > 0 ? per_sm : 1);
   return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
 }
 
-cudaError_t launch_batch_compress(const BatchDev& d, uint32_t count, uint64_t total_groups,
-                                  uint64_t max_blocks, const BatchCfg& c, cudaStream_t s) {
+cudaError_t launch_batch_compress(const BatchDev& d, uint32_t count, const uint64_t groups[3],
+                                  uint64_t max_blocks, const BatchCfg& c, cudaStream_t s,
+                                  cudaEvent_t* marks) {
+  if (marks) cudaEventRecord(marks[0], s);
   batch_begin_kernel<<<(count + 255) / 256 + 1, 256, 0, s>>>(d.states, count, d.ctrl);
-  batch_map_kernel<<<grid_of(c, kStageMap, div_up_u64(total_groups, kBWarps)), kBThreads,
-                     sizeof(BatchMapSmem), s>>>(d.items, d.states, count, total_groups, d.ctrl,
-                                                d.group_flags);
+  if (groups[1])
+    batch_map_kernel<MANS_U16><<<grid_of(c, kStageMap, div_up_u64(groups[1], kBWarps), c.occ_u16_map),
+                                 kBThreads, 0, s>>>(d.items, d.states, count, groups[1], d.ctrl,
+                                                    d.group_flags, d.hists, d.hist_items);
+  if (groups[2])
+    batch_map_kernel<MANS_U32><<<grid_of(c, kStageMap, div_up_u64(groups[2], kBWarps)), kBThreads,
+                                 sizeof(BatchMapSmem), s>>>(d.items, d.states, count, groups[2],
+                                                            d.ctrl, d.group_flags, d.hists,
+                                                            d.hist_items);
+  if (groups[0])
+    batch_map_kernel<MANS_U8><<<grid_of(c, kStageMap, div_up_u64(groups[0], kBWarps), c.occ_u8_map),
+                                kBThreads, 0, s>>>(d.items, d.states, count, groups[0], d.ctrl,
+                                                   d.group_flags, d.hists, d.hist_items);
+  if (marks) cudaEventRecord(marks[1], s);
   batch_plan_encode_kernel<<<grid_of(c, kStagePlanEnc, count), 256, 0, s>>>(
-      d.items, d.states, count, d.ctrl, d.item_flags);
+      d.items, d.states, count, d.ctrl, d.item_flags, d.hists, d.hist_items);
+  if (marks) cudaEventRecord(marks[2], s);
   batch_encode_kernel<<<grid_of(c, kStageEncode, div_up_u64(max_blocks, kBWarps)), kBThreads,
                         sizeof(BatchEncSmem), s>>>(d.items, d.states, count, d.ctrl,
                                                    d.block_flags, d.slots);
+  if (marks) cudaEventRecord(marks[3], s);
   return cudaGetLastError();
 }
 
-cudaError_t launch_batch_decompress(const BatchDev& d, uint32_t count, uint64_t total_groups,
-                                    uint64_t max_chunks, const BatchCfg& c, cudaStream_t s) {
+cudaError_t launch_batch_decompress(const BatchDev& d, uint32_t count, const uint64_t groups[3],
+                                    uint64_t max_chunks, const BatchCfg& c, cudaStream_t s,
+                                    cudaEvent_t* marks) {
+  if (marks) cudaEventRecord(marks[0], s);
   batch_begin_kernel<<<(count + 255) / 256 + 1, 256, 0, s>>>(d.states, count, d.ctrl);
   batch_plan_decode_kernel<<<grid_of(c, kStagePlanDec, count), 32, 0, s>>>(
       d.items, d.states, count, d.ctrl, d.item_flags);
+  if (marks) cudaEventRecord(marks[1], s);
   batch_decode_kernel<<<grid_of(c, kStageDecode, max_chunks), kBThreads, sizeof(BatchDecSmem),
                         s>>>(d.items, d.states, count, d.ctrl);
-  batch_unmap_kernel<<<grid_of(c, kStageUnmap, div_up_u64(total_groups, kBWarps)), kBThreads,
-                       sizeof(BatchUnmapSmem), s>>>(d.items, d.states, count, total_groups, d.ctrl);
+  if (marks) cudaEventRecord(marks[2], s);
+  if (groups[1])
+    batch_unmap_kernel<MANS_U16><<<grid_of(c, kStageUnmap, div_up_u64(groups[1], kBWarps),
+                                           c.occ_u16_unmap),
+                                   kBThreads, 0, s>>>(d.items, d.states, count, groups[1], d.ctrl);
+  if (groups[2])
+    batch_unmap_kernel<MANS_U32><<<grid_of(c, kStageUnmap, div_up_u64(groups[2], kBWarps)),
+                                   kBThreads, sizeof(BatchUnmapSmem), s>>>(d.items, d.states, count,
+                                                                          groups[2], d.ctrl);
+  if (marks) cudaEventRecord(marks[3], s);
   return cudaGetLastError();
 }
 

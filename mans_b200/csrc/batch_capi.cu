@@ -14,6 +14,7 @@ using namespace mans;
 namespace {
 constexpr int kStagingRing = 2;
 constexpr int kCaptureSlots = 4;
+constexpr int kTimingRing = 64;
 constexpr uint64_t kItemSlack = 4096 + 64;
 constexpr uint64_t kMaxMerged = 0xfffffff0ull;  // rANS header counts are u32
 
@@ -46,14 +47,20 @@ struct mans_batch {
   LaunchCfg lcfg;
   BatchCfg cfg;
   uint32_t last_count = 0;
+  // opt-in stage timing: four events per recorded call (ring of kTimingRing
+  // compress and kTimingRing decompress calls); never used under capture
+  bool timing = false;
+  cudaEvent_t marks[2][kTimingRing][4] = {};
+  int recorded[2] = {0, 0};
 };
 
 namespace {
 
 // Lay out one call's buffers: fills `h` (count descriptors) and the totals.
 mans_status layout(mans_batch* b, const mans_batch_item* items, uint32_t count, bool compress,
-                   BatchItem* h, uint64_t* total_groups, uint64_t* max_units) {
-  uint64_t off = 0, groups = 0, units = 0, total = 0;
+                   BatchItem* h, uint64_t groups[3], uint64_t* max_units, uint64_t* max_chunks) {
+  uint64_t off = 0, flags = 0, units = 0, chunks = 0, total = 0;
+  groups[0] = groups[1] = groups[2] = 0;
   for (uint32_t i = 0; i < count; ++i) {
     const mans_batch_item& it = items[i];
     const uint64_t eb = elem_bytes((uint32_t)it.dtype);
@@ -74,30 +81,37 @@ mans_status layout(mans_batch* b, const mans_batch_item* items, uint32_t count, 
     d.out_cap = it.out_capacity;
     d.dtype = (uint32_t)it.dtype;
     d.prob_bits = compress ? (uint32_t)it.precision : 0u;
-    d.group_base = groups;
+    const int kind = dtype_kind(d.dtype);
+    d.group_base = groups[kind];
+    d.flag_base = flags;
+    uint64_t g = 0, blocks = 0;
     if (it.dtype == MANS_U8) {
       if (bytes > kMaxMerged) return MANS_ERR_TOO_LARGE;
       d.m = nullptr;
       d.m_cap = 0;
       // compress: histogram chunks; decompress: no inverse mapping
-      if (compress) groups += div_up_u64(bytes, 4096);
-      units += div_up_u64(bytes, kAnsBlock);
+      if (compress) g = div_up_u64(bytes, 4096);
+      blocks = div_up_u64(bytes, kAnsBlock);
     } else {
-      const uint64_t g = div_up_u64(it.n_elems, kAdmGroup);
+      g = div_up_u64(it.n_elems, kAdmGroup);
       const uint64_t hdr = it.dtype == MANS_U16 ? 6 * g : 40 * g;
       const uint64_t cap = std::min(mapped_cap(bytes, b->ratio_pct), kMaxMerged);
       d.m = b->pool + off + merged_pad(hdr);
       d.m_cap = cap;
       off += align_up(cap + kItemSlack, 256);
-      groups += g;
-      units += div_up_u64(cap, kAnsBlock);
+      blocks = div_up_u64(cap, kAnsBlock);
     }
+    groups[kind] += g;
+    flags += g;
+    units += blocks;
+    chunks += div_up_u64(blocks, 8);
   }
-  if (total > b->max_total_bytes || off > b->pool_bytes || groups > b->group_flags_n ||
-      units > b->block_flags_n)
+  if (total > b->max_total_bytes || off > b->pool_bytes || flags > b->group_flags_n ||
+      units > b->block_flags_n || groups[0] >= (1ull << 32) || groups[1] >= (1ull << 32) ||
+      groups[2] >= (1ull << 32))
     return MANS_ERR_TOO_LARGE;
-  *total_groups = groups;
   *max_units = units;
+  *max_chunks = chunks;
   return MANS_OK;
 }
 
@@ -136,15 +150,22 @@ mans_status run(mans_batch* b, const mans_batch_item* items, uint32_t count, boo
   if (count > b->max_items) return MANS_ERR_TOO_LARGE;
   if (count == 0) return MANS_OK;
   std::vector<BatchItem> h(count);
-  uint64_t groups = 0, units = 0;
-  mans_status st = layout(b, items, count, compress, h.data(), &groups, &units);
+  uint64_t groups[3], units = 0, chunks = 0;
+  mans_status st = layout(b, items, count, compress, h.data(), groups, &units, &chunks);
   if (st != MANS_OK) return st;
   st = upload(b, h.data(), count, s);
   if (st != MANS_OK) return st;
   b->last_count = count;
-  cudaError_t e = compress ? launch_batch_compress(b->dev, count, groups, units, b->cfg, s)
-                           : launch_batch_decompress(b->dev, count, groups,
-                                                     div_up_u64(units, 8), b->cfg, s);
+  cudaEvent_t* marks = nullptr;
+  const int dir = compress ? 0 : 1;
+  if (b->timing && b->recorded[dir] < kTimingRing) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cap);
+    if (cap == cudaStreamCaptureStatusNone) marks = b->marks[dir][b->recorded[dir]++];
+  }
+  cudaError_t e = compress ? launch_batch_compress(b->dev, count, groups, units, b->cfg, s, marks)
+                           : launch_batch_decompress(b->dev, count, groups, chunks, b->cfg, s,
+                                                     marks);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
 }
 
@@ -170,7 +191,7 @@ extern "C" {
 
 mans_status mans_batch_create(mans_batch** out, uint32_t max_items, uint64_t max_total_bytes,
                               uint32_t merged_ratio_pct) {
-  if (!out || max_items == 0) return MANS_ERR_INVALID_ARG;
+  if (!out || max_items == 0 || max_items >= (1u << 20)) return MANS_ERR_INVALID_ARG;
   if (merged_ratio_pct == 0) merged_ratio_pct = 210;
   if (merged_ratio_pct < 50 || merged_ratio_pct > 10000) return MANS_ERR_INVALID_ARG;
   *out = nullptr;
@@ -191,7 +212,9 @@ mans_status mans_batch_create(mans_batch** out, uint32_t max_items, uint64_t max
   const uint64_t o_ctrl = 0;
   const uint64_t o_items = align_up(sizeof(Ctrl), 256);
   const uint64_t o_states = align_up(o_items + sizeof(BatchItem) * (uint64_t)max_items, 256);
-  const uint64_t o_iflags = align_up(o_states + sizeof(BatchState) * (uint64_t)max_items, 256);
+  const uint64_t o_hists = align_up(o_states + sizeof(BatchState) * (uint64_t)max_items, 256);
+  const uint64_t o_iflags =
+      align_up(o_hists + 4ull * kAnsSyms * kHistCopies * (uint64_t)max_items, 256);
   const uint64_t o_gflags = align_up(o_iflags + 8ull * max_items, 256);
   const uint64_t o_bflags = align_up(o_gflags + 8 * b->group_flags_n, 256);
   const uint64_t o_slots = align_up(o_bflags + 8 * b->block_flags_n, 256);
@@ -210,6 +233,8 @@ mans_status mans_batch_create(mans_batch** out, uint32_t max_items, uint64_t max
   b->dev.ctrl = reinterpret_cast<Ctrl*>(b->base + o_ctrl);
   b->dev.items = reinterpret_cast<BatchItem*>(b->base + o_items);
   b->dev.states = reinterpret_cast<BatchState*>(b->base + o_states);
+  b->dev.hists = reinterpret_cast<uint32_t*>(b->base + o_hists);
+  b->dev.hist_items = max_items;
   b->dev.item_flags = reinterpret_cast<unsigned long long*>(b->base + o_iflags);
   b->dev.group_flags = reinterpret_cast<unsigned long long*>(b->base + o_gflags);
   b->dev.block_flags = reinterpret_cast<unsigned long long*>(b->base + o_bflags);
@@ -238,6 +263,10 @@ mans_status mans_batch_destroy(mans_batch* b) {
   cudaSetDevice(b->device);
   for (auto& e : b->staged)
     if (e) cudaEventDestroy(e);
+  for (auto& dir : b->marks)
+    for (auto& call : dir)
+      for (auto& e : call)
+        if (e) cudaEventDestroy(e);
   for (auto& p : b->staging)
     if (p) cudaFreeHost(p);
   cudaError_t e = b->base ? cudaFree(b->base) : cudaSuccess;
@@ -278,6 +307,38 @@ mans_status mans_batch_status(mans_batch* b, mans_stream_t stream, uint32_t* ite
     }
   }
   return (mans_status)first;
+}
+
+mans_status mans_batch_set_timing(mans_batch* b, int enable) {
+  if (!b) return MANS_ERR_INVALID_ARG;
+  if (enable && !b->marks[0][0][0]) {
+    for (auto& dir : b->marks)
+      for (auto& call : dir)
+        for (auto& e : call)
+          if (cudaEventCreate(&e) != cudaSuccess) return MANS_ERR_CUDA;
+  }
+  b->timing = enable != 0;
+  b->recorded[0] = b->recorded[1] = 0;
+  return MANS_OK;
+}
+
+mans_status mans_batch_stage_times(mans_batch* b, float ms[6], int calls[2]) {
+  if (!b || !ms) return MANS_ERR_INVALID_ARG;
+  for (int k = 0; k < 6; ++k) ms[k] = 0.f;
+  for (int dir = 0; dir < 2; ++dir) {
+    for (int c = 0; c < b->recorded[dir]; ++c) {
+      cudaEvent_t* m = b->marks[dir][c];
+      if (cudaEventSynchronize(m[3]) != cudaSuccess) return MANS_ERR_CUDA;
+      for (int k = 0; k < 3; ++k) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, m[k], m[k + 1]) != cudaSuccess) return MANS_ERR_CUDA;
+        ms[3 * dir + k] += t;
+      }
+    }
+    if (calls) calls[dir] = b->recorded[dir];
+    b->recorded[dir] = 0;
+  }
+  return MANS_OK;
 }
 
 mans_status mans_batch_get_schedule(const mans_batch* b, int ctas_per_sm[6], int max_ctas_per_sm[6]) {

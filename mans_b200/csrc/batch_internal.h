@@ -21,14 +21,14 @@ struct BatchItem {
   uint64_t out_cap;              // compress: stream capacity
   uint8_t* m;                    // mapped bytes (per-element section 16-byte aligned)
   uint64_t m_cap;
-  uint64_t group_base;           // first global mapping unit of this buffer
+  uint64_t group_base;           // first mapping unit of this buffer in its dtype's unit space
+  uint64_t flag_base;            // first look-back flag of this buffer's groups
   uint32_t dtype;                // MANS_U8 / MANS_U16 / MANS_U32
   uint32_t prob_bits;
 };
 
 // Per-buffer device state (kept in the batch workspace).
 struct BatchState {
-  uint32_t hist[256];
   uint2 enc[256];
   uint32_t pdf[256];
   unsigned long long msize;   // mapped bytes (compress) / decoded bytes (decompress)
@@ -39,10 +39,17 @@ struct BatchState {
   uint32_t n_hdr, cw, p;      // decompress: header fields
 };
 
+// Each buffer's histogram is kept in kHistCopies copies (CTA b adds into copy
+// b % kHistCopies), which spreads the merge atomics over more L2 slices; the
+// plan stage sums them. Copy c of buffer i: hists + (c * hist_items + i) * 256.
+constexpr int kHistCopies = 4;
+
 struct BatchDev {
   Ctrl* ctrl;
   BatchItem* items;
   BatchState* states;
+  uint32_t* hists;
+  uint32_t hist_items;
   unsigned long long* item_flags;
   unsigned long long* group_flags;
   unsigned long long* block_flags;
@@ -65,13 +72,23 @@ struct BatchCfg {
   int sms = 148;
   int occ[kStages] = {1, 1, 1, 1, 1, 1};
   int ctas_per_sm[kStages] = {1, 1, 1, 1, 1, 1};
+  // occupancy of the lighter map / unmap variants (grids scale with it)
+  int occ_u16_map = 1, occ_u8_map = 1, occ_u16_unmap = 1;
 };
 
 void init_batch_cfg(BatchCfg& c, const LaunchCfg& base);
 uint64_t batch_slot_bytes(const BatchCfg& c);
-cudaError_t launch_batch_compress(const BatchDev& d, uint32_t count, uint64_t total_groups,
-                                  uint64_t max_blocks, const BatchCfg& c, cudaStream_t s);
-cudaError_t launch_batch_decompress(const BatchDev& d, uint32_t count, uint64_t total_groups,
-                                    uint64_t max_chunks, const BatchCfg& c, cudaStream_t s);
+// marks (optional): four events recorded before the first kernel and after
+// each stage (compress: map, plan, encode; decompress: plan, decode, unmap).
+// groups[k]: mapping units of the buffers of dtype kind k (0: MANS_U8
+// histogram chunks, 1: MANS_U16 groups, 2: MANS_U32 groups); each kind has
+// its own unit space and its own launch of the map (unmap) stage.
+cudaError_t launch_batch_compress(const BatchDev& d, uint32_t count, const uint64_t groups[3],
+                                  uint64_t max_blocks, const BatchCfg& c, cudaStream_t s,
+                                  cudaEvent_t* marks = nullptr);
+cudaError_t launch_batch_decompress(const BatchDev& d, uint32_t count, const uint64_t groups[3],
+                                    uint64_t max_chunks, const BatchCfg& c, cudaStream_t s,
+                                    cudaEvent_t* marks = nullptr);
+inline int dtype_kind(uint32_t dtype) { return dtype == 1 ? 0 : dtype == 2 ? 1 : 2; }
 
 }  // namespace mans
