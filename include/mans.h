@@ -202,6 +202,78 @@ mans_status mans_batch_set_schedule(mans_batch* b, const int ctas_per_sm[6]);
 mans_status mans_batch_autotune(mans_batch* b, const mans_batch_item* items, uint32_t count,
                                 mans_stream_t stream, float* best_ms);
 
+/* ------------------------------------------------------------------------
+ * Serving loop: a scheduler thread inside the library admits mixed compress
+ * and decompress requests against an HBM budget and folds whatever is queued
+ * into the next batched launch (continuous batching: several launches per
+ * direction are in flight on their own streams, and requests that arrive
+ * meanwhile form the next ones). All device memory the server holds -- batch
+ * workspaces and an arena for results -- is allocated at creation within the
+ * budget. The reference has no serving form; each result is byte-identical to
+ * mans_compress / mans_decompress of that request alone.
+ * ---------------------------------------------------------------------- */
+typedef struct mans_server mans_server;
+
+typedef enum mans_op { MANS_OP_COMPRESS = 0, MANS_OP_DECOMPRESS = 1 } mans_op;
+
+typedef struct mans_server_config {
+  uint64_t hbm_budget_bytes;  /* device memory the server may hold */
+  uint64_t max_batch_bytes;   /* uncompressed bytes of one launch, and of one request
+                                 (0 = budget / 8) */
+  uint32_t max_batch_items;   /* requests of one launch (0 = 1024) */
+  uint32_t lanes;             /* launches in flight per direction (0 = 2; plain: 1) */
+  uint32_t merged_ratio_pct;  /* mapped-byte room per buffer, see mans_batch_create */
+  int plain;                  /* 1: one request per launch through mans_compress /
+                                 mans_decompress (the per-request baseline) */
+} mans_server_config;
+
+typedef struct mans_request {
+  mans_op op;
+  mans_dtype dtype;
+  int precision;          /* compress: 9..11 */
+  uint32_t pad;
+  uint64_t n_elems;       /* uncompressed elements */
+  const void* d_in;       /* device; compress: values, decompress: stream (16-byte aligned) */
+  uint64_t in_bytes;      /* decompress: stream bytes */
+  void* d_out;            /* caller-owned device output, or NULL for one from the arena */
+  uint64_t out_capacity;  /* bytes at d_out */
+  uint64_t tag;           /* returned in the completion */
+  uint64_t arrival_ns;    /* arrival time on mans_clock_ns() (0 = at submission) */
+} mans_request;
+
+typedef struct mans_completion {
+  uint64_t ticket;
+  uint64_t tag;
+  mans_status status;     /* this request's own status */
+  uint32_t batch_items;   /* requests in the launch that served it */
+  uint64_t detail;
+  void* d_out;            /* the result (device); arena results stay valid until released */
+  uint64_t out_bytes;     /* stream bytes (compress) or value bytes (decompress) */
+  uint64_t queued_ns;     /* arrival -> launch */
+  uint64_t latency_ns;    /* arrival -> completion seen by the scheduler */
+} mans_completion;
+
+typedef struct mans_server_stats {
+  uint64_t submitted, completed, launches, in_flight, queued;
+  uint64_t arena_bytes, arena_used, arena_peak, device_bytes;
+} mans_server_stats;
+
+/* Monotonic clock of the server (ns), for arrival_ns. */
+uint64_t mans_clock_ns(void);
+mans_status mans_server_create(mans_server** s, const mans_server_config* cfg);
+/* Finishes every submitted request, then frees everything. */
+mans_status mans_server_destroy(mans_server* s);
+/* Validates and queues a request (MANS_ERR_TOO_LARGE when it can never fit). */
+mans_status mans_server_submit(mans_server* s, const mans_request* r, uint64_t* ticket);
+/* Up to max completions; waits up to timeout_us for the first (0 = no wait). */
+mans_status mans_server_poll(mans_server* s, mans_completion* out, uint32_t max, uint32_t* n,
+                             uint32_t timeout_us);
+/* Returns an arena result's memory to the server. */
+mans_status mans_server_release(mans_server* s, uint64_t ticket);
+mans_status mans_server_get_stats(mans_server* s, mans_server_stats* out);
+/* Diagnostic: the server's arena allocator on the host (no device memory). */
+uint64_t mans_debug_arena(uint64_t size, const uint64_t* ops, uint32_t n_ops, uint64_t* results);
+
 /* Library version string. */
 const char* mans_version(void);
 

@@ -65,6 +65,14 @@ SIGNATURES = {
     "mans_batch_get_schedule": (_i32, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "mans_batch_set_schedule": (_i32, [_vp, C.POINTER(C.c_int)]),
     "mans_batch_autotune": (_i32, [_vp, _vp, _u32, _vp, C.POINTER(C.c_float)]),
+    "mans_clock_ns": (_u64, []),
+    "mans_server_create": (_i32, [C.POINTER(_vp), _vp]),
+    "mans_server_destroy": (_i32, [_vp]),
+    "mans_server_submit": (_i32, [_vp, _vp, C.POINTER(_u64)]),
+    "mans_server_poll": (_i32, [_vp, _vp, _u32, C.POINTER(_u32), _u32]),
+    "mans_server_release": (_i32, [_vp, _u64]),
+    "mans_server_get_stats": (_i32, [_vp, _vp]),
+    "mans_debug_arena": (_u64, [_u64, _vp, _u32, _vp]),
     "mans_version": (C.c_char_p, []),
     "mans_debug_enc_entry": (None, [_u32, _u32, _i32, C.POINTER(_u32)]),
 }

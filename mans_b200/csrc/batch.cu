@@ -598,6 +598,25 @@ __global__ __launch_bounds__(kBThreads) void batch_unmap_kernel(const BatchItem*
 }
 
 // ------------------------------------------------------------------------
+// Gather every buffer's status and detail into compact arrays (for an
+// asynchronous copy to the host).
+// ------------------------------------------------------------------------
+__global__ void batch_gather_status_kernel(const BatchState* states, uint32_t count,
+                                           uint32_t* status, unsigned long long* detail) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    status[i] = states[i].status;
+    detail[i] = states[i].detail;
+  }
+}
+
+cudaError_t launch_batch_gather_status(const BatchDev& d, uint32_t count, uint32_t* status,
+                                       unsigned long long* detail, cudaStream_t s) {
+  const unsigned grid = (unsigned)((count + 255) / 256 > 0 ? (count + 255) / 256 : 1);
+  batch_gather_status_kernel<<<grid, 256, 0, s>>>(d.states, count, status, detail);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
 // Host launchers
 // ------------------------------------------------------------------------
 static int occ(const void* fn, int threads, size_t smem) {

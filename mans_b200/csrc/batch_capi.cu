@@ -49,6 +49,8 @@ struct mans_batch {
   uint32_t last_count = 0;
   // opt-in stage timing: four events per recorded call (ring of kTimingRing
   // compress and kTimingRing decompress calls); never used under capture
+  uint32_t* d_status = nullptr;           // gathered statuses (device)
+  unsigned long long* d_detail = nullptr;  // gathered details (device)
   bool timing = false;
   cudaEvent_t marks[2][kTimingRing][4] = {};
   int recorded[2] = {0, 0};
@@ -187,6 +189,23 @@ __global__ void batch_checksum_kernel(const BatchItem* items, const BatchState* 
 
 }  // namespace
 
+namespace mans {
+mans_status batch_enqueue_status(mans_batch* b, uint32_t count, uint32_t* host_status,
+                                 uint64_t* host_detail, cudaStream_t s) {
+  if (!b || count > b->max_items) return MANS_ERR_INVALID_ARG;
+  if (count == 0) return MANS_OK;
+  if (launch_batch_gather_status(b->dev, count, b->d_status, b->d_detail, s) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  if (host_status && cudaMemcpyAsync(host_status, b->d_status, 4ull * count,
+                                     cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  if (host_detail && cudaMemcpyAsync(host_detail, b->d_detail, 8ull * count,
+                                     cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  return MANS_OK;
+}
+}  // namespace mans
+
 extern "C" {
 
 mans_status mans_batch_create(mans_batch** out, uint32_t max_items, uint64_t max_total_bytes,
@@ -218,7 +237,8 @@ mans_status mans_batch_create(mans_batch** out, uint32_t max_items, uint64_t max
   const uint64_t o_gflags = align_up(o_iflags + 8ull * max_items, 256);
   const uint64_t o_bflags = align_up(o_gflags + 8 * b->group_flags_n, 256);
   const uint64_t o_slots = align_up(o_bflags + 8 * b->block_flags_n, 256);
-  const uint64_t o_pool = align_up(o_slots + batch_slot_bytes(b->cfg), 256);
+  const uint64_t o_gather = align_up(o_slots + batch_slot_bytes(b->cfg), 256);
+  const uint64_t o_pool = align_up(o_gather + 12ull * max_items, 256);
   b->bytes = align_up(o_pool + b->pool_bytes, 256);
   if (cudaMalloc(&b->base, b->bytes) != cudaSuccess) {
     cudaGetLastError();
@@ -240,6 +260,8 @@ mans_status mans_batch_create(mans_batch** out, uint32_t max_items, uint64_t max
   b->dev.block_flags = reinterpret_cast<unsigned long long*>(b->base + o_bflags);
   b->dev.slots = b->base + o_slots;
   b->pool = b->base + o_pool;
+  b->d_detail = reinterpret_cast<unsigned long long*>(b->base + o_gather);
+  b->d_status = reinterpret_cast<uint32_t*>(b->base + o_gather + 8ull * max_items);
   for (int k = 0; k < kStagingRing + kCaptureSlots; ++k) {
     if (cudaMallocHost(&b->staging[k], sizeof(BatchItem) * (uint64_t)max_items) != cudaSuccess) {
       mans_batch_destroy(b);

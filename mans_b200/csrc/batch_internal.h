@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "mans_internal.h"
+#include "../../include/mans.h"
 
 namespace mans {
 
@@ -89,6 +90,20 @@ cudaError_t launch_batch_compress(const BatchDev& d, uint32_t count, const uint6
 cudaError_t launch_batch_decompress(const BatchDev& d, uint32_t count, const uint64_t groups[3],
                                     uint64_t max_chunks, const BatchCfg& c, cudaStream_t s,
                                     cudaEvent_t* marks = nullptr);
+cudaError_t launch_batch_gather_status(const BatchDev& d, uint32_t count, uint32_t* status,
+                                       unsigned long long* detail, cudaStream_t s);
 inline int dtype_kind(uint32_t dtype) { return dtype == 1 ? 0 : dtype == 2 ? 1 : 2; }
 
+}  // namespace mans
+
+namespace mans {
+// Enqueue on s: copy the first `count` buffers' statuses and details of the
+// batch's last call into host (pinned) arrays. For the serving loop.
+mans_status batch_enqueue_status(mans_batch* b, uint32_t count, uint32_t* host_status,
+                                 uint64_t* host_detail, cudaStream_t s);
+// The same for a single-buffer workspace (one call); also clears its status.
+mans_status workspace_enqueue_status(mans_workspace* ws, uint32_t* host_status,
+                                     uint64_t* host_detail, cudaStream_t s);
+// Worst-case rANS stream bytes of n input bytes.
+uint64_t ans_stream_bound(uint64_t n);
 }  // namespace mans

@@ -102,6 +102,22 @@ uint64_t ans_bound(uint64_t n) {
 
 }  // namespace
 
+namespace mans {
+// Enqueue on s: copy the workspace's device status and detail into host
+// (pinned) memory, then clear them for the next call. For the serving loop.
+mans_status workspace_enqueue_status(mans_workspace* ws, uint32_t* host_status,
+                                     uint64_t* host_detail, cudaStream_t s) {
+  if (!ws) return MANS_ERR_INVALID_ARG;
+  if (cudaMemcpyAsync(host_status, &ws->ctrl->status, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(host_detail, &ws->ctrl->detail, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemsetAsync(&ws->ctrl->status, 0, 4, s) != cudaSuccess ||
+      cudaMemsetAsync(&ws->ctrl->detail, 0, 8, s) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  return MANS_OK;
+}
+uint64_t ans_stream_bound(uint64_t n) { return ans_bound(n); }
+}  // namespace mans
+
 extern "C" {
 
 const char* mans_version(void) { return "mans_b200 0.1.0 (sm_100a)"; }
