@@ -62,7 +62,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mans", "reference"], default="mans")
-    ap.add_argument("--workload", choices=list(WORKLOADS) + ["mixed_c3"], default="detector_u32")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["mixed_c3", "serve_c5"],
+                    default="detector_u32")
+    ap.add_argument("--requests", type=int, default=0, help="serve_c5: requests (100000)")
+    ap.add_argument("--corpus", type=int, default=0, help="serve_c5: distinct buffers (256)")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve_c5: offered GB/s")
+    ap.add_argument("--saturation-requests", type=int, default=4000)
+    ap.add_argument("--no-check", action="store_true", help="serve_c5: skip the per-result check")
     ap.add_argument("--items", type=int, default=0, help="mixed_c3: number of buffers (4096)")
     ap.add_argument("--merged-ratio", type=int, default=120,
                     help="mixed_c3: mapped-byte room per buffer, percent of its bytes")
@@ -815,6 +821,167 @@ def run_mixed(args):
         print(json.dumps(result), flush=True)
 
 
+# ---------------------------------------------------------------- serving
+SERVE_DESC = ("serve_c5: {R} requests, Poisson arrivals at {rate:g} GB/s offered, sizes log-uniform "
+              "in [16 KiB, 256 MiB] (a seeded corpus of {D} buffers, alternating uint16 gradients and "
+              "uint32 Laplace codes as in mixed_c3), 50/50 compress/decompress, decompress inputs are "
+              "earlier compress outputs of the same buffers; 64 GiB HBM budget; seed 5")
+
+
+def serve_trace(srv, reqs, arrivals_s, corpus, streams, check: bool):
+    """Submit reqs at their arrival times (a submitter thread) and collect,
+    check and release every completion. Returns per-request records."""
+    import torch
+
+    from mans_b200 import serve
+    R = len(reqs)
+    t0 = serve.clock_ns() + 50_000_000
+    err = []
+
+    def submitter():
+        try:
+            for k, (op, i) in enumerate(reqs):
+                target = t0 + int(arrivals_s[k] * 1e9)
+                now = serve.clock_ns()
+                if target > now + 200_000:
+                    time.sleep((target - now) / 1e9)
+                x, code, n = corpus[i]
+                if op == 0:
+                    srv.submit(serve.COMPRESS, code, n, x.data_ptr(), precision=10, tag=k,
+                               arrival_ns=target)
+                else:
+                    s = streams[i]
+                    srv.submit(serve.DECOMPRESS, code, n, s.data_ptr(), in_bytes=s.numel(), tag=k,
+                               arrival_ns=target)
+        except Exception as e:  # pragma: no cover - reported below
+            err.append(e)
+
+    th = threading.Thread(target=submitter, daemon=True)
+    th.start()
+    rec = np.zeros((R, 5), dtype=np.float64)  # latency ns, queued ns, batch items, ok, done time ns
+    n = 0
+    bad = 0
+    while n < R:
+        if err:
+            raise err[0]
+        for c in srv.poll(timeout_us=5000):
+            k = c.tag
+            op, i = reqs[k]
+            ok = c.status == 0
+            if ok and check:
+                if op == 0:
+                    ref = streams[i]
+                    ok = c.out_bytes == ref.numel() and bool(torch.equal(serve.view_device(c.d_out, c.out_bytes), ref))
+                else:
+                    x = corpus[i][0].view(torch.uint8)
+                    ok = c.out_bytes == x.numel() and bool(torch.equal(serve.view_device(c.d_out, c.out_bytes), x))
+            if c.status == 0:
+                srv.release(c.ticket)
+            bad += 0 if ok else 1
+            rec[k] = (c.latency_ns, c.queued_ns, c.batch_items, 1.0 if ok else 0.0, serve.clock_ns() - t0)
+            n += 1
+    th.join()
+    return rec, bad
+
+
+def serve_summary(rec, reqs, sizes_b, arrivals_s):
+    lat = rec[:, 0] / 1e6
+    ops = np.array([op for op, _ in reqs])
+    nbytes = np.array([sizes_b[i] for _, i in reqs], dtype=np.float64)
+    span = rec[:, 4].max() / 1e9  # last completion, from the trace's time origin
+    first = float(arrivals_s[0])
+    out = {"p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+           "mean_ms": round(float(lat.mean()), 3),
+           "compress_p50_ms": round(float(np.percentile(lat[ops == 0], 50)), 3) if (ops == 0).any() else None,
+           "compress_p99_ms": round(float(np.percentile(lat[ops == 0], 99)), 3) if (ops == 0).any() else None,
+           "decompress_p50_ms": round(float(np.percentile(lat[ops == 1], 50)), 3) if (ops == 1).any() else None,
+           "decompress_p99_ms": round(float(np.percentile(lat[ops == 1], 99)), 3) if (ops == 1).any() else None,
+           "queued_p50_ms": round(float(np.percentile(rec[:, 1] / 1e6, 50)), 3),
+           "mean_batch_items": round(float(rec[:, 2].mean()), 2),
+           "aggregate_gbs": round(float(nbytes.sum() / max(span - first, 1e-9) / 1e9), 3),
+           "requests": len(reqs), "bytes": int(nbytes.sum()), "all_identical": bool(rec[:, 3].all())}
+    return out
+
+
+def run_serve(args):
+    import torch
+
+    import mans_b200 as mb
+    from mans_b200 import serve
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    R = args.requests or 100_000
+    D = args.corpus or 256
+    rate = args.rate
+    rng = np.random.default_rng(5)
+    sz = np.exp(rng.uniform(np.log(16 << 10), np.log(256 << 20), D))
+    sz = (np.floor(sz / 1024) * 1024).astype(np.int64)
+    ab = rng.uniform(-1000, 1000, (D, 2))
+    items, off = [], 0
+    for i, nb in enumerate(sz.tolist()):
+        elem = 2 if i % 2 == 0 else 4
+        items.append({"elem": elem, "n": nb // elem, "bytes": nb // elem * elem, "off": off,
+                      "a": float(ab[i, 0]), "b": float(ab[i, 1])})
+        off += (nb + 255) // 256 * 256
+    pool = gen_mixed_device(items, off, seed=5 + rank)
+    tdt = {2: torch.uint16, 4: torch.uint32}
+    corpus = [(pool[it["off"]:it["off"] + it["bytes"]].view(tdt[it["elem"]]),
+               mb.MANS_U16 if it["elem"] == 2 else mb.MANS_U32, it["n"]) for it in items]
+    sizes_b = [it["bytes"] for it in items]
+    # compressed corpus through the single-buffer path (the reference result of every request)
+    ws = mb.Workspace(max(sizes_b))
+    streams = [mb.compress(x, 10, ws=ws) for x, _, _ in corpus]
+    ws.close()
+    ops = (rng.random(R) < 0.5).astype(np.int64)
+    idx = rng.integers(0, D, R)
+    reqs = [(int(o), int(i)) for o, i in zip(ops, idx)]
+    mean_b = float(np.mean([sizes_b[i] for i in idx]))
+    lam = rate * 1e9 / mean_b
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, R))
+    budget = 64 << 30
+    results = {}
+    R_sat = min(R, args.saturation_requests)
+    for name, kw in (("batched", dict(max_batch_bytes=1 << 30, max_batch_items=1024, lanes=2,
+                                      merged_ratio_pct=args.merged_ratio)),
+                     ("plain", dict(max_batch_bytes=max(sizes_b), plain=True))):
+        srv = serve.Server(budget, **kw)
+        dev_bytes = srv.stats()["device_bytes"]
+        clk = ClockSampler(local)
+        with clk:
+            rec, bad = serve_trace(srv, reqs, arrivals, corpus, streams, check=not args.no_check)
+        st = srv.stats()
+        summ = serve_summary(rec, reqs, sizes_b, arrivals)
+        summ.update({"launches": st["launches"], "arena_peak_bytes": st["arena_peak"],
+                     "device_bytes": dev_bytes, "mismatches": bad, "clocks": clk.summary()})
+        # saturation: every request of a prefix queued at once
+        rec2, bad2 = serve_trace(srv, reqs[:R_sat], np.zeros(R_sat), corpus, streams, check=False)
+        s2 = serve_summary(rec2, reqs[:R_sat], sizes_b, np.zeros(R_sat))
+        summ["saturated"] = {"requests": R_sat, "aggregate_gbs": s2["aggregate_gbs"],
+                             "p50_ms": s2["p50_ms"], "p99_ms": s2["p99_ms"],
+                             "mean_batch_items": s2["mean_batch_items"], "errors": bad2}
+        srv.close()
+        results[name] = summ
+    b, p = results["batched"], results["plain"]
+    line = {
+        "metric": METRIC, "value": b["aggregate_gbs"], "unit": "GB/s", "n_gpus": world,
+        "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16+u32", "data": "synthetic",
+        "config": {"workload": SERVE_DESC.format(R=R, rate=rate, D=D), "offered_gbs": rate,
+                   "arrival_rate_per_s": round(lam, 1), "hbm_budget_bytes": budget,
+                   "parallelism": "single GPU"},
+        "p50_ms": b["p50_ms"], "p99_ms": b["p99_ms"],
+        "batched": b, "plain": p,
+        "p99_plain_over_batched": round(p["p99_ms"] / b["p99_ms"], 3) if b["p99_ms"] else None,
+        "saturated_batched_vs_plain": round(b["saturated"]["aggregate_gbs"] / p["saturated"]["aggregate_gbs"], 3),
+        "bit_exact": b["all_identical"] and p["all_identical"],
+        "e2e": None, "e2e_note": "requests reference device-resident buffers; see mixed_c3 / default runs for host-buffer e2e",
+        "gpu_launches": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def check_oracle(args, x, s) -> bool:
     from oracle import pyoracle as O
     from tests.helpers import to_host
@@ -843,6 +1010,8 @@ def main():
         run_reference(args)
     elif args.workload == "mixed_c3":
         run_mixed(args)
+    elif args.workload == "serve_c5":
+        run_serve(args)
     else:
         run_mans(args)
 
