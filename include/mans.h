@@ -101,6 +101,40 @@ mans_status mans_decompress(mans_workspace* ws, mans_dtype dtype, const void* d_
                             mans_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * On-disk compatibility layouts of the uint16 mapped buffer. NATIVE is the
+ * V15 merged layout for MANS_U16 (mapping/nv/mappingV15_fused_uint16.cu
+ * :933-957) and the decodable record layout for MANS_U32. V12 replaces the
+ * i32 prefix header by u16 group lengths (mappingV12_bit-adm-thrust-prefixsum.cu
+ * :606-634; lanes past n are 0xFF); CPUV2 writes g + 1 prefix words, the last
+ * one the total (mapping/cpu/mappingcpuV2.cpp:117-121, 271-285). The layout
+ * changes the mapped bytes and so the stream; decode with the same layout.
+ * ---------------------------------------------------------------------- */
+typedef enum mans_layout {
+  MANS_LAYOUT_NATIVE = 0,
+  MANS_LAYOUT_V12 = 1,   /* MANS_U16 only */
+  MANS_LAYOUT_CPUV2 = 2  /* MANS_U16 only */
+} mans_layout;
+
+mans_status mans_compress_ex(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                             const void* d_in, uint64_t n_elems, void* d_out,
+                             uint64_t out_capacity, uint64_t* d_out_size, int precision,
+                             mans_stream_t stream);
+mans_status mans_decompress_ex(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                               const void* d_in, uint64_t in_size, void* d_out, uint64_t n_elems,
+                               mans_stream_t stream);
+/* The mapping alone: d_out receives the mapped buffer exactly as the
+ * reference's mapping programs write it to disk (for MANS_U32 the record
+ * layout, whose records section is mappingV9_fuse.cu's output), and
+ * *d_out_size (device, u64) its size. MANS_U16 / MANS_U32 only. */
+mans_status mans_adm_map(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                         const void* d_in, uint64_t n_elems, void* d_out, uint64_t out_capacity,
+                         uint64_t* d_out_size, mans_stream_t stream);
+/* Inverse of mans_adm_map: in_size mapped bytes at d_in back to n_elems values. */
+mans_status mans_adm_unmap(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                           const void* d_in, uint64_t in_size, void* d_out, uint64_t n_elems,
+                           mans_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Reference-compatible rANS entry points (include/ans, src/GpuANS.cu). Same
  * arguments and meaning as the reference; they run on a library-owned
  * workspace per (device, stream) that is created on first use, so the first

@@ -47,6 +47,10 @@ SIGNATURES = {
     "mans_max_compressed_size": (_u64, [_i32, _u64]),
     "mans_compress": (_i32, [_vp, _i32, _vp, _u64, _vp, _u64, _vp, _i32, _vp]),
     "mans_decompress": (_i32, [_vp, _i32, _vp, _u64, _vp, _u64, _vp]),
+    "mans_compress_ex": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp, _i32, _vp]),
+    "mans_decompress_ex": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp]),
+    "mans_adm_map": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp, _vp]),
+    "mans_adm_unmap": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp]),
     "mans_ans_encode": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
     "mans_ans_decode": (_i32, [_i32, _vp, _vp, _vp]),
     "mans_ans_encode_batch": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
@@ -189,25 +193,69 @@ class Workspace:
             pass
 
 
-def compress_into(ws: Workspace, x, out, out_size, precision: int = 10, stream=None) -> None:
+# mans_layout: mapped-buffer layouts (uint16 compatibility modes)
+LAYOUT_NATIVE, LAYOUT_V12, LAYOUT_CPUV2 = 0, 1, 2
+
+
+def compress_into(ws: Workspace, x, out, out_size, precision: int = 10, stream=None,
+                  layout: int = LAYOUT_NATIVE) -> None:
     """Enqueue MANS compress of device tensor x into out (uint8) and out_size (int64[1])."""
     n = x.numel()
     code = dtype_code(x)
-    _check(load().mans_compress(ws.h, code, x.data_ptr() if n else None, n, out.data_ptr(),
-                                out.numel(), out_size.data_ptr(), precision,
-                                _stream_handle(stream)), "mans_compress")
+    _check(load().mans_compress_ex(ws.h, code, layout, x.data_ptr() if n else None, n,
+                                   out.data_ptr(), out.numel(), out_size.data_ptr(), precision,
+                                   _stream_handle(stream)), "mans_compress")
 
 
-def decompress_into(ws: Workspace, stream_bytes, in_size: int, out, stream=None) -> None:
+def decompress_into(ws: Workspace, stream_bytes, in_size: int, out, stream=None,
+                    layout: int = LAYOUT_NATIVE) -> None:
     """Enqueue MANS decompress of stream_bytes[:in_size] into out (dtype decides the mapping)."""
     n = out.numel()
     code = dtype_code(out)
-    _check(load().mans_decompress(ws.h, code, stream_bytes.data_ptr(), in_size,
-                                  out.data_ptr() if n else None, n, _stream_handle(stream)),
+    _check(load().mans_decompress_ex(ws.h, code, layout, stream_bytes.data_ptr(), in_size,
+                                     out.data_ptr() if n else None, n, _stream_handle(stream)),
            "mans_decompress")
 
 
-def compress(x, precision: int = 10, ws: Optional[Workspace] = None, stream=None):
+def adm_map(x, layout: int = LAYOUT_NATIVE, ws: Optional[Workspace] = None, stream=None):
+    """The mapped buffer of device tensor x (uint16/uint32) as the reference's mappers write it."""
+    torch = _torch()
+    n = x.numel()
+    own = ws is None
+    if own:
+        ws = Workspace(max(n * x.element_size(), 1))
+    cap = n * x.element_size() * 3 + 65536
+    out = torch.empty(cap, dtype=torch.uint8, device=x.device)
+    size = torch.zeros(1, dtype=torch.int64, device=x.device)
+    _check(load().mans_adm_map(ws.h, dtype_code(x), layout, x.data_ptr() if n else None, n,
+                               out.data_ptr(), cap, size.data_ptr(), _stream_handle(stream)),
+           "mans_adm_map")
+    ws.check(stream, "mans_adm_map")
+    res = out[: int(size.item())].clone()
+    if own:
+        ws.close()
+    return res
+
+
+def adm_unmap(m, n: int, dtype, layout: int = LAYOUT_NATIVE, ws: Optional[Workspace] = None,
+              stream=None):
+    """Inverse of adm_map: n values of dtype from the mapped buffer m (device uint8)."""
+    torch = _torch()
+    out = torch.empty(n, dtype=dtype, device=m.device)
+    own = ws is None
+    if own:
+        ws = Workspace(max(n * out.element_size(), 1))
+    _check(load().mans_adm_unmap(ws.h, dtype_code(out), layout, m.data_ptr(), m.numel(),
+                                 out.data_ptr() if n else None, n, _stream_handle(stream)),
+           "mans_adm_unmap")
+    ws.check(stream, "mans_adm_unmap")
+    if own:
+        ws.close()
+    return out
+
+
+def compress(x, precision: int = 10, ws: Optional[Workspace] = None, stream=None,
+             layout: int = LAYOUT_NATIVE):
     """Compress device tensor x (uint8/uint16/uint32); returns a uint8 tensor (synchronises)."""
     torch = _torch()
     n = x.numel()
@@ -218,7 +266,7 @@ def compress(x, precision: int = 10, ws: Optional[Workspace] = None, stream=None
     cap = max_compressed_size(code, n)
     out = torch.empty(cap, dtype=torch.uint8, device=x.device)
     size = torch.zeros(1, dtype=torch.int64, device=x.device)
-    compress_into(ws, x, out, size, precision, stream)
+    compress_into(ws, x, out, size, precision, stream, layout)
     ws.check(stream, "mans_compress")
     nbytes = int(size.item())
     res = out[:nbytes].clone()
@@ -227,14 +275,15 @@ def compress(x, precision: int = 10, ws: Optional[Workspace] = None, stream=None
     return res
 
 
-def decompress(s, n: int, dtype, ws: Optional[Workspace] = None, stream=None):
+def decompress(s, n: int, dtype, ws: Optional[Workspace] = None, stream=None,
+               layout: int = LAYOUT_NATIVE):
     """Decompress a stream (device uint8 tensor) of n elements of dtype (synchronises)."""
     torch = _torch()
     out = torch.empty(n, dtype=dtype, device=s.device)
     own = ws is None
     if own:
         ws = Workspace(max(n * out.element_size(), 1))
-    decompress_into(ws, s, s.numel(), out, stream)
+    decompress_into(ws, s, s.numel(), out, stream, layout)
     ws.check(stream, "mans_decompress")
     if own:
         ws.close()

@@ -33,15 +33,31 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
+CLI = os.path.join(HERE, "mans_cli")
+CLI_SRC = os.path.join(HERE, "cli", "mans_cli.cu")
+
+
+def build_cli(force: bool = False) -> str:
+    """The command-line driver, linked against the library (found next to it)."""
+    if not force and os.path.exists(CLI) and os.path.getmtime(CLI) >= max(
+            os.path.getmtime(CLI_SRC), os.path.getmtime(LIB)):
+        return CLI
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-o", LIB, *sources()]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
+    cmd = [nvcc, *ARCH, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-o", CLI,
+           CLI_SRC, "-L", HERE, "-lmans_b200", "-Xlinker", "-rpath,$ORIGIN"]
     subprocess.run(cmd, check=True)
+    return CLI
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or not up_to_date():
+        nvcc = os.environ.get("NVCC", "nvcc")
+        cmd = [nvcc, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-o", LIB, *sources()]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    build_cli(force)
     return LIB
 
 

@@ -10,6 +10,7 @@ namespace mans {
 // group's look-back), and the group one grid of warps ahead is prefetched
 // into L2 for whichever warp claims it. The group's bit offset comes from a
 // decoupled look-back over per-group flags.
+template <int kLayout>
 __global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
     const uint16_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ M, uint64_t m_cap,
     Ctrl* ctrl, unsigned long long* flags, int prob_bits) {
@@ -29,19 +30,22 @@ __global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
       const uint64_t ns = ((uint64_t)grp + ahead) * kAdmGroup;
       prefetch_l2(in + ns, (uint32_t)(2 * min_u64(kAdmGroup, n - ns)));
     }
-    map16_group(in, n, M, m_cap, flags, &ctrl->merged_size, grp, epoch, sink, s_h[warp], lane);
+    map16_group<kLayout>(in, n, M, m_cap, flags, &ctrl->merged_size, grp, epoch, sink, s_h[warp],
+                         lane);
   }
   hist_merge_and_normalize(s_h, kMapWarps, ctrl, g == 0 ? 0ull : ~0ull, 0, prob_bits);
 }
 
+template <int kLayout>
 __global__ __launch_bounds__(kUnmapThreads, 4) void adm_u16_unmap_kernel(
-    const uint8_t* __restrict__ M, uint64_t n, uint16_t* __restrict__ out, Ctrl* ctrl) {
+    const uint8_t* __restrict__ M, uint64_t n, uint16_t* __restrict__ out, Ctrl* ctrl,
+    const uint32_t* __restrict__ v12_excl) {
   const Sink sink = sink_of(ctrl);
   if (sink_failed(sink)) return;
   const int lane = threadIdx.x & 31;
   const uint64_t g = div_up_u64(n, kAdmGroup);
   const uint64_t msize = __ldcg(&ctrl->merged_size);
-  const uint64_t bits_base = 6 * g + n;
+  const uint64_t bits_base = u16_header_bytes(kLayout, g) + n;
   if (msize < bits_base || ((msize - bits_base) & 31)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) report(sink, MANS_ERR_CORRUPT, msize);
     return;
@@ -50,33 +54,123 @@ __global__ __launch_bounds__(kUnmapThreads, 4) void adm_u16_unmap_kernel(
   const uint64_t warps = (uint64_t)gridDim.x * (kUnmapThreads / 32);
   for (uint64_t grp = (uint64_t)blockIdx.x * (kUnmapThreads / 32) + (threadIdx.x >> 5); grp < g;
        grp += warps)
-    unmap16_group(M, n, tot, out, grp, sink, lane);
+    unmap16_group<kLayout>(M, n, tot, out, grp, sink, lane, v12_excl);
+}
+
+// V12 layout: exclusive prefix of the u16 group lengths into excl (tiles of
+// 2,048 groups, one per CTA of 256 threads, claimed in order; single-pass
+// look-back over per-tile flags). The last CTA advances the epoch, because
+// the flags are shared with the rANS encoder.
+constexpr int kScanThreads = 256, kScanPer = 8, kScanTile = kScanThreads * kScanPer;
+
+__global__ __launch_bounds__(kScanThreads) void adm_u16_v12_scan_kernel(
+    const uint8_t* __restrict__ M, uint64_t n, uint32_t* __restrict__ excl, Ctrl* ctrl,
+    unsigned long long* flags) {
+  __shared__ uint32_t s_tile, s_warp[kScanThreads / 32], s_prefix;
+  __shared__ int s_last;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const uint64_t g = div_up_u64(n, kAdmGroup);
+  const uint16_t* len = reinterpret_cast<const uint16_t*>(M);
+  const uint32_t epoch = *((volatile uint32_t*)&ctrl->epoch);
+  const Sink sink = sink_of(ctrl);
+  while (true) {
+    __syncthreads();
+    if (t == 0) s_tile = atomicAdd(&ctrl->tile_counter[6], 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t base = (uint64_t)tile * kScanTile;
+    if (base >= g) break;
+    uint32_t v[kScanPer], sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanPer; ++i) {
+      const uint64_t k = base + (uint64_t)t * kScanPer + i;
+      v[i] = k < g ? len[k] : 0u;
+      sum += v[i];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0, total = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w) {
+      if (w < warp) wbase += s_warp[w];
+      total += s_warp[w];
+    }
+    if (warp == 0) {
+      if (lane == 0) st_flag(&flags[tile], make_flag(tile == 0 ? kFlagIncl : kFlagAgg, epoch, total));
+      uint32_t pre = 0;
+      if (tile > 0) {
+        pre = lookback_exclusive(flags, tile, epoch, sink);
+        if (lane == 0) st_flag(&flags[tile], make_flag(kFlagIncl, epoch, pre + total));
+      }
+      if (lane == 0) s_prefix = pre;
+    }
+    __syncthreads();
+    uint32_t run = s_prefix + wbase + incl - sum;
+#pragma unroll
+    for (int i = 0; i < kScanPer; ++i) {
+      const uint64_t k = base + (uint64_t)t * kScanPer + i;
+      if (k < g) excl[k] = run;
+      run += v[i];
+    }
+  }
+  __syncthreads();
+  if (t == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctrl->done_counter[6], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && t == 0) {
+    ctrl->tile_counter[6] = 0;
+    ctrl->done_counter[6] = 0;
+    ctrl->epoch = (epoch + 1) & 0x3fffffffu;
+  }
 }
 
 // ------------------------------------------------------------------------
 void init_adm_u16_launch_cfg(LaunchCfg& cfg) {
   int nmap = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nmap, adm_u16_map_kernel, kMapThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nmap, adm_u16_map_kernel<kLayoutV15>, kMapThreads,
+                                                0);
   cfg.map_ctas = nmap > 0 ? nmap : 1;
 }
 
 cudaError_t launch_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* m, uint64_t m_cap,
                                Ctrl* ctrl, unsigned long long* flags, int prob_bits,
-                               const LaunchCfg& cfg, cudaStream_t s) {
+                               const LaunchCfg& cfg, cudaStream_t s, int layout) {
   const uint64_t ctas = div_up_u64(div_up_u64(n, kAdmGroup), kMapWarps);
   const uint64_t cap = (uint64_t)cfg.sms * cfg.map_ctas;
   const unsigned grid = (unsigned)(ctas < 1 ? 1 : (ctas < cap ? ctas : cap));
-  adm_u16_map_kernel<<<grid, kMapThreads, 0, s>>>(in, n, m, m_cap, ctrl, flags, prob_bits);
+  if (layout == kLayoutV12)
+    adm_u16_map_kernel<kLayoutV12><<<grid, kMapThreads, 0, s>>>(in, n, m, m_cap, ctrl, flags, prob_bits);
+  else if (layout == kLayoutCpuV2)
+    adm_u16_map_kernel<kLayoutCpuV2><<<grid, kMapThreads, 0, s>>>(in, n, m, m_cap, ctrl, flags, prob_bits);
+  else
+    adm_u16_map_kernel<kLayoutV15><<<grid, kMapThreads, 0, s>>>(in, n, m, m_cap, ctrl, flags, prob_bits);
   return cudaGetLastError();
 }
 
 cudaError_t launch_adm_u16_unmap(const uint8_t* m, uint64_t n, uint16_t* out, Ctrl* ctrl,
-                                 const LaunchCfg& cfg, cudaStream_t s) {
+                                 const LaunchCfg& cfg, cudaStream_t s, int layout,
+                                 uint32_t* v12_excl, unsigned long long* scan_flags) {
   const uint64_t groups = div_up_u64(n, kAdmGroup);
   const uint64_t want = div_up_u64(groups, kUnmapThreads / 32);
   const uint64_t cap = (uint64_t)cfg.sms * 8;
   const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
-  adm_u16_unmap_kernel<<<grid, kUnmapThreads, 0, s>>>(m, n, out, ctrl);
+  if (layout == kLayoutV12) {
+    const uint64_t tiles = div_up_u64(groups, kScanTile);
+    const unsigned sgrid = (unsigned)(tiles < 1 ? 1 : (tiles < (uint64_t)cfg.sms * 4 ? tiles : cfg.sms * 4));
+    adm_u16_v12_scan_kernel<<<sgrid, kScanThreads, 0, s>>>(m, n, v12_excl, ctrl, scan_flags);
+    adm_u16_unmap_kernel<kLayoutV12><<<grid, kUnmapThreads, 0, s>>>(m, n, out, ctrl, v12_excl);
+  } else if (layout == kLayoutCpuV2) {
+    adm_u16_unmap_kernel<kLayoutCpuV2><<<grid, kUnmapThreads, 0, s>>>(m, n, out, ctrl, nullptr);
+  } else {
+    adm_u16_unmap_kernel<kLayoutV15><<<grid, kUnmapThreads, 0, s>>>(m, n, out, ctrl, nullptr);
+  }
   return cudaGetLastError();
 }
 

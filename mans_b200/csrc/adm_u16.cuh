@@ -12,6 +12,13 @@
 //   to its lane's bit stream (MSB first); the group length L is the longest
 //   lane in bytes; a shorter lane's final partial byte is filled with 1s.
 // Merged: [i32 exclusive L prefix x g][u16 center x g][u8 code x n][bits].
+// Compatibility layouts (same codes and bits) replace the length header:
+//   kLayoutV12   [u16 L x g] (mappingV12_bit-adm-thrust-prefixsum.cu
+//                :606-634; a lane holding no element is 0xFF in all its L
+//                bytes, since V12's concat (:405-428) skips it in a buffer
+//                filled with 255 (:504));
+//   kLayoutCpuV2 [i32 L prefix x (g + 1), the last = total]
+//                (mapping/cpu/mappingcpuV2.cpp:117-121, 271-285).
 //
 // B200 organisation: each warp maps one group at a time, groups handed out
 // in order by an atomic counter. The group-length prefix is a single-pass
@@ -25,6 +32,16 @@
 #include "ans_table.cuh"
 
 namespace mans {
+
+constexpr int kLayoutV15 = 0, kLayoutV12 = 1, kLayoutCpuV2 = 2;
+
+// Bytes before the centers and before the codes, for g groups.
+__host__ __device__ constexpr uint64_t u16_len_bytes(int layout, uint64_t g) {
+  return layout == kLayoutV12 ? 2 * g : layout == kLayoutCpuV2 ? 4 * g + 4 : 4 * g;
+}
+__host__ __device__ constexpr uint64_t u16_header_bytes(int layout, uint64_t g) {
+  return u16_len_bytes(layout, g) + 2 * g;
+}
 
 constexpr int kMapWarps = kAdmGroupsPerTile;  // 8
 constexpr int kMapThreads = kMapWarps * 32;   // 256
@@ -76,6 +93,7 @@ __device__ __forceinline__ void load_lane_u16(const uint16_t* __restrict__ in, u
 // Map group `grp` of one buffer (one warp). flags: the buffer's per-group
 // look-back flags; msize_out: written by the buffer's last group; hist: the
 // warp's shared histogram.
+template <int kLayout = kLayoutV15>
 __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uint64_t n,
                                             uint8_t* __restrict__ M, uint64_t m_cap,
                                             unsigned long long* flags,
@@ -83,11 +101,12 @@ __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uin
                                             uint32_t epoch, const Sink& sink, uint32_t* hist,
                                             int lane) {
   const uint64_t g = div_up_u64(n, kAdmGroup);
+  const uint64_t hdr = u16_header_bytes(kLayout, g);
   uint8_t* p_len = M;
-  uint8_t* p_ctr = M + 4 * g;
-  uint8_t* p_code = M + 6 * g;
-  uint8_t* p_bits = M + 6 * g + n;
-  const uint64_t bits_base = 6 * g + n;  // offset of the bits section in M
+  uint8_t* p_ctr = M + u16_len_bytes(kLayout, g);
+  uint8_t* p_code = M + hdr;
+  uint8_t* p_bits = M + hdr + n;
+  const uint64_t bits_base = hdr + n;  // offset of the bits section in M
   uint32_t w[8];
   load_lane_u16(in, n, grp, lane, w);
 
@@ -132,13 +151,17 @@ __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uin
     for (int i = 0; i < 16; ++i)
       if (i < cnt) p_code[ls + i] = (uint8_t)(codes[i >> 2] >> ((i & 3) * 8));
   }
-  // bit bytes of a short lane (< 64 bits): tail fill and histogram now
+  // bit bytes of a short lane (< 64 bits): tail fill and histogram now. In
+  // the V12 layout a lane without elements is all 0xFF.
   const bool fast = pos < 64;
+  const bool v12_empty = kLayout == kLayoutV12 && cnt == 0;
+  const uint32_t rest = v12_empty ? 0xffu : 0u;  // bytes past the first 8
   if (fast) {
-    if (pos < 8 * L) acc |= tail_fill_mask(pos);
+    if (v12_empty) acc = ~0ull;
+    else if (pos < 8 * L) acc |= tail_fill_mask(pos);
     const uint32_t nb8 = L < 8 ? L : 8u;
     for (uint32_t b = 0; b < nb8; ++b) atomicAdd(&hist[(uint32_t)(acc >> (56 - 8 * b)) & 0xffu], 1u);
-    if (L > 8) atomicAdd(&hist[0], L - 8);
+    if (L > 8) atomicAdd(&hist[rest], L - 8);
   }
 
   // ---- group bit offset (in units of 32 bytes)
@@ -153,15 +176,31 @@ __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uin
     if (msize > m_cap) report(sink, MANS_ERR_WORKSPACE_OVERFLOW, msize);
   }
 
-  // lengths (i32, written as two u16: M is only 2-byte aligned here) and center
+  // lengths (i32 written as two u16: M is only 2-byte aligned here, or u16 L)
+  // and center
   if (lane == 0) {
-    reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[0] = (uint16_t)(gexcl & 0xffffu);
-    reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[1] = (uint16_t)(gexcl >> 16);
+    if constexpr (kLayout == kLayoutV12) {
+      reinterpret_cast<uint16_t*>(p_len + 2ull * grp)[0] = (uint16_t)L;
+      atomicAdd(&hist[L & 0xff], 1u);
+      atomicAdd(&hist[(L >> 8) & 0xff], 1u);
+    } else {
+      reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[0] = (uint16_t)(gexcl & 0xffffu);
+      reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[1] = (uint16_t)(gexcl >> 16);
+      atomicAdd(&hist[gexcl & 0xff], 1u);
+      atomicAdd(&hist[(gexcl >> 8) & 0xff], 1u);
+      atomicAdd(&hist[(gexcl >> 16) & 0xff], 1u);
+      atomicAdd(&hist[gexcl >> 24], 1u);
+      if (kLayout == kLayoutCpuV2 && (uint64_t)grp + 1 == g) {
+        const uint32_t tot = gexcl + L;  // the CPU layout's extra final prefix word
+        reinterpret_cast<uint16_t*>(p_len + 4ull * g)[0] = (uint16_t)(tot & 0xffffu);
+        reinterpret_cast<uint16_t*>(p_len + 4ull * g)[1] = (uint16_t)(tot >> 16);
+        atomicAdd(&hist[tot & 0xff], 1u);
+        atomicAdd(&hist[(tot >> 8) & 0xff], 1u);
+        atomicAdd(&hist[(tot >> 16) & 0xff], 1u);
+        atomicAdd(&hist[tot >> 24], 1u);
+      }
+    }
     reinterpret_cast<uint16_t*>(p_ctr + 2ull * grp)[0] = (uint16_t)c;
-    atomicAdd(&hist[gexcl & 0xff], 1u);
-    atomicAdd(&hist[(gexcl >> 8) & 0xff], 1u);
-    atomicAdd(&hist[(gexcl >> 16) & 0xff], 1u);
-    atomicAdd(&hist[gexcl >> 24], 1u);
     atomicAdd(&hist[c & 0xff], 1u);
     atomicAdd(&hist[(c >> 8) & 0xff], 1u);
   }
@@ -171,7 +210,7 @@ __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uin
     uint8_t* dst = p_bits + 32ull * gexcl + (uint64_t)lane * L;
     if (fast) {
       for (uint32_t b = 0; b < L; ++b)
-        dst[b] = (uint8_t)(b < 8 ? (uint32_t)(acc >> (56 - 8 * b)) & 0xffu : 0u);
+        dst[b] = (uint8_t)(b < 8 ? (uint32_t)(acc >> (56 - 8 * b)) & 0xffu : rest);
     } else {
       // Long lane: regenerate the stream byte by byte.
       uint32_t cur = 0, bi = 0, bp = 0;
@@ -218,19 +257,35 @@ __device__ __forceinline__ uint32_t rd_u32_2aligned(const uint8_t* p) {
   return (uint32_t)q[0] | ((uint32_t)q[1] << 16);
 }
 
-// Restore group `grp` of one buffer (one warp). msize: the merged size
-// recorded by the decoder; tot: bit bytes / 32 (validated by the caller).
+// Restore group `grp` of one buffer (one warp). tot: bit bytes / 32
+// (validated by the caller). V12 layout: v12_excl holds the exclusive prefix
+// of its u16 lengths (computed by the caller).
+template <int kLayout = kLayoutV15>
 __device__ __forceinline__ void unmap16_group(const uint8_t* __restrict__ M, uint64_t n,
                                               uint64_t tot, uint16_t* __restrict__ out,
-                                              uint64_t grp, const Sink& sink, int lane) {
+                                              uint64_t grp, const Sink& sink, int lane,
+                                              const uint32_t* v12_excl = nullptr) {
   const uint64_t g = div_up_u64(n, kAdmGroup);
-  const uint64_t bits_base = 6 * g + n;
+  const uint64_t bits_base = u16_header_bytes(kLayout, g) + n;
   const uint8_t* p_len = M;
-  const uint8_t* p_ctr = M + 4 * g;
-  const uint8_t* p_code = M + 6 * g;
+  const uint8_t* p_ctr = M + u16_len_bytes(kLayout, g);
+  const uint8_t* p_code = M + u16_header_bytes(kLayout, g);
   const uint8_t* p_bits = M + bits_base;
-  const uint64_t ex = rd_u32_2aligned(p_len + 4 * grp);
-  const uint64_t nx = grp + 1 < g ? rd_u32_2aligned(p_len + 4 * (grp + 1)) : tot;
+  uint64_t ex, nx;
+  if constexpr (kLayout == kLayoutV12) {
+    ex = __ldg(v12_excl + grp);
+    nx = ex + reinterpret_cast<const uint16_t*>(p_len)[grp];
+  } else {
+    ex = rd_u32_2aligned(p_len + 4 * grp);
+    nx = grp + 1 < g ? rd_u32_2aligned(p_len + 4 * (grp + 1)) : tot;
+  }
+  // the layouts that record the total must agree with the decoded size
+  const bool last = grp + 1 == g;
+  if ((kLayout == kLayoutV12 && last && nx != tot) ||
+      (kLayout == kLayoutCpuV2 && last && rd_u32_2aligned(p_len + 4 * g) != tot)) {
+    if (lane == 0) report(sink, MANS_ERR_CORRUPT, grp);
+    return;
+  }
   if (ex > nx || nx > tot) {
     if (lane == 0) report(sink, MANS_ERR_CORRUPT, grp);
     return;

@@ -41,6 +41,7 @@ struct mans_workspace {
   uint64_t ans_flags_n = 0;
   uint8_t* merged = nullptr;  // 16-byte aligned region of merged_cap + slack bytes
   uint8_t* enc_slots = nullptr;  // per-warp word slots of the encode kernel
+  uint32_t* v12_excl = nullptr;  // group offsets of the V12 layout's unmap
   LaunchCfg cfg;
   // Opt-in kernel timing: a ring of event triples per recorded call
   // (compress: start, after mapping, after encode; decompress: start, after
@@ -118,6 +119,146 @@ mans_status workspace_enqueue_status(mans_workspace* ws, uint32_t* host_status,
 uint64_t ans_stream_bound(uint64_t n) { return ans_bound(n); }
 }  // namespace mans
 
+namespace {
+
+// Copy the mapped bytes (size in ctrl) out of the workspace, with a capacity
+// check; thread 0 stores the size.
+__global__ void export_merged_kernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
+                                     uint64_t cap, Ctrl* ctrl, unsigned long long* out_size) {
+  if (*((volatile uint32_t*)&ctrl->status) != 0) return;
+  const uint64_t n = __ldcg(&ctrl->merged_size);
+  if (n > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) report_error(ctrl, MANS_ERR_OUTPUT_OVERFLOW, n);
+    return;
+  }
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0 && out_size) *out_size = n;
+}
+
+// Copy caller-supplied mapped bytes into the workspace and record their size.
+__global__ void import_merged_kernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
+                                     uint64_t n, Ctrl* ctrl) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->merged_size = n;
+}
+
+unsigned copy_grid(const LaunchCfg& cfg, uint64_t n) {
+  const uint64_t want = div_up_u64(n, 256 * 16);
+  const uint64_t cap = (uint64_t)cfg.sms * 8;
+  return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+}
+
+bool valid_layout(mans_dtype dtype, mans_layout layout) {
+  if (layout == MANS_LAYOUT_NATIVE) return true;
+  return dtype == MANS_U16 && (layout == MANS_LAYOUT_V12 || layout == MANS_LAYOUT_CPUV2);
+}
+
+mans_status compress_impl(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                          const void* d_in, uint64_t n_elems, void* d_out, uint64_t out_capacity,
+                          uint64_t* d_out_size, int precision, mans_stream_t stream,
+                          bool map_only) {
+  if (!ws || !d_out || !d_out_size || (!d_in && n_elems)) return MANS_ERR_INVALID_ARG;
+  const uint64_t eb = elem_bytes(dtype);
+  if (eb == 0 || !valid_layout(dtype, layout)) return MANS_ERR_INVALID_ARG;
+  if (!valid_precision(precision)) return MANS_ERR_UNSUPPORTED_PRECISION;
+  if ((d_in && !aligned16(d_in)) || !aligned16(d_out)) return MANS_ERR_ALIGNMENT;
+  const uint64_t in_bytes = n_elems * eb;
+  if (in_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  unsigned long long* osz = reinterpret_cast<unsigned long long*>(d_out_size);
+  cudaError_t e = cudaSuccess;
+  if (dtype == MANS_U8 && in_bytes > kMaxMerged) return MANS_ERR_TOO_LARGE;
+  uint8_t* m = nullptr;
+  mark(ws, 0, s);
+  if (dtype == MANS_U8) {
+    e = launch_hist_bytes((const uint8_t*)d_in, in_bytes, ws->ctrl, precision, ws->cfg, s);
+    mark(ws, 1, s);
+    if (e == cudaSuccess)
+      e = launch_ans_encode((const uint8_t*)d_in, (uint8_t*)d_out, out_capacity, osz, nullptr,
+                            ws->ctrl, ws->ans_flags, precision,
+                            div_up_u64(in_bytes, kAnsBlock), ws->cfg, s, ws->enc_slots);
+    mark(ws, 2, s);
+    return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+  }
+  if (dtype == MANS_U16) {
+    const uint64_t hdr = adm_u16_header_bytes(n_elems, (int)layout);
+    const uint64_t g = div_up_u64(n_elems, kAdmGroup);
+    if (hdr + n_elems + 32 * g > ws->merged_cap) return MANS_ERR_TOO_LARGE;
+    m = ws->merged + merged_pad(hdr);
+    e = launch_adm_u16_map((const uint16_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
+                           ws->adm_flags, precision, ws->cfg, s, (int)layout);
+  } else {
+    const uint64_t hdr = adm_u32_header_bytes(n_elems);
+    if (hdr + n_elems > ws->merged_cap) return MANS_ERR_TOO_LARGE;
+    m = ws->merged + merged_pad(hdr);
+    e = launch_adm_u32_map((const uint32_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
+                           ws->adm_flags, precision, ws->cfg, s);
+  }
+  mark(ws, 1, s);
+  if (e == cudaSuccess) {
+    if (map_only) {
+      export_merged_kernel<<<copy_grid(ws->cfg, ws->merged_cap), 256, 0, s>>>(
+          m, (uint8_t*)d_out, out_capacity, ws->ctrl, osz);
+      e = cudaGetLastError();
+    } else {
+      e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
+                            ws->ans_flags, precision, div_up_u64(ws->merged_cap, kAnsBlock),
+                            ws->cfg, s, ws->enc_slots);
+    }
+  }
+  mark(ws, 2, s);
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+mans_status decompress_impl(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                            const void* d_in, uint64_t in_size, void* d_out, uint64_t n_elems,
+                            mans_stream_t stream, bool unmap_only) {
+  if (!ws || !d_in || (!d_out && n_elems)) return MANS_ERR_INVALID_ARG;
+  const uint64_t eb = elem_bytes(dtype);
+  if (eb == 0 || !valid_layout(dtype, layout)) return MANS_ERR_INVALID_ARG;
+  if (!aligned16(d_in) || (d_out && !aligned16(d_out))) return MANS_ERR_ALIGNMENT;
+  const uint64_t out_bytes = n_elems * eb;
+  if (out_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaSuccess;
+  mark(ws, 3, s);
+  if (dtype == MANS_U8) {
+    e = launch_ans_decode((const uint8_t*)d_in, in_size, (uint8_t*)d_out, out_bytes, ws->ctrl, -1,
+                          0, div_up_u64(out_bytes, kAnsBlock), ws->cfg, s);
+    mark(ws, 4, s);
+    mark(ws, 5, s);
+    return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+  }
+  const uint64_t hdr = dtype == MANS_U16 ? adm_u16_header_bytes(n_elems, (int)layout)
+                                         : adm_u32_header_bytes(n_elems);
+  uint8_t* m = ws->merged + merged_pad(hdr);
+  if (unmap_only) {
+    if (in_size > ws->merged_cap) return MANS_ERR_TOO_LARGE;
+    import_merged_kernel<<<copy_grid(ws->cfg, in_size), 256, 0, s>>>((const uint8_t*)d_in, m,
+                                                                      in_size, ws->ctrl);
+    e = cudaGetLastError();
+  } else {
+    e = launch_ans_decode((const uint8_t*)d_in, in_size, m, ws->merged_cap, ws->ctrl, -1, 1,
+                          div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
+  }
+  mark(ws, 4, s);
+  if (e == cudaSuccess) {
+    if (dtype == MANS_U16)
+      e = launch_adm_u16_unmap(m, n_elems, (uint16_t*)d_out, ws->ctrl, ws->cfg, s, (int)layout,
+                               ws->v12_excl, ws->ans_flags);
+    else
+      e = launch_adm_u32_unmap(m, n_elems, (uint32_t*)d_out, ws->ctrl, ws->cfg, s);
+  }
+  mark(ws, 5, s);
+  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* mans_version(void) { return "mans_b200 0.1.0 (sm_100a)"; }
@@ -145,7 +286,8 @@ mans_status mans_workspace_create(mans_workspace** out, uint64_t max_input_bytes
   const uint64_t off_adm = align_up(sizeof(Ctrl), 256);
   const uint64_t off_ans = align_up(off_adm + 8 * ws->adm_flags_n, 256);
   const uint64_t off_slots = align_up(off_ans + 8 * ws->ans_flags_n, 256);
-  const uint64_t off_m = align_up(off_slots + ans_encode_slot_bytes(ws->cfg), 256);
+  const uint64_t off_v12 = align_up(off_slots + ans_encode_slot_bytes(ws->cfg), 256);
+  const uint64_t off_m = align_up(off_v12 + 4 * ws->adm_flags_n, 256);
   ws->bytes = align_up(off_m + merged_capacity + kSlack, 256);
   if (cudaMalloc(&ws->base, ws->bytes) != cudaSuccess) {
     cudaGetLastError();
@@ -161,6 +303,7 @@ mans_status mans_workspace_create(mans_workspace** out, uint64_t max_input_bytes
   ws->adm_flags = reinterpret_cast<unsigned long long*>(ws->base + off_adm);
   ws->ans_flags = reinterpret_cast<unsigned long long*>(ws->base + off_ans);
   ws->enc_slots = ws->base + off_slots;
+  ws->v12_excl = reinterpret_cast<uint32_t*>(ws->base + off_v12);
   ws->merged = ws->base + off_m;
   *out = ws;
   return MANS_OK;
@@ -216,88 +359,44 @@ uint64_t mans_max_compressed_size(mans_dtype dtype, uint64_t n_elems) {
 mans_status mans_compress(mans_workspace* ws, mans_dtype dtype, const void* d_in,
                           uint64_t n_elems, void* d_out, uint64_t out_capacity,
                           uint64_t* d_out_size, int precision, mans_stream_t stream) {
-  if (!ws || !d_out || !d_out_size || (!d_in && n_elems)) return MANS_ERR_INVALID_ARG;
-  const uint64_t eb = elem_bytes(dtype);
-  if (eb == 0) return MANS_ERR_INVALID_ARG;
-  if (!valid_precision(precision)) return MANS_ERR_UNSUPPORTED_PRECISION;
-  if ((d_in && !aligned16(d_in)) || !aligned16(d_out)) return MANS_ERR_ALIGNMENT;
-  const uint64_t in_bytes = n_elems * eb;
-  if (in_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  unsigned long long* osz = reinterpret_cast<unsigned long long*>(d_out_size);
-  cudaError_t e = cudaSuccess;
-  if (dtype == MANS_U8 && in_bytes > kMaxMerged) return MANS_ERR_TOO_LARGE;
-  mark(ws, 0, s);
-  if (dtype == MANS_U8) {
-    e = launch_hist_bytes((const uint8_t*)d_in, in_bytes, ws->ctrl, precision, ws->cfg, s);
-    mark(ws, 1, s);
-    if (e == cudaSuccess)
-      e = launch_ans_encode((const uint8_t*)d_in, (uint8_t*)d_out, out_capacity, osz, nullptr,
-                            ws->ctrl, ws->ans_flags, precision,
-                            div_up_u64(in_bytes, kAnsBlock), ws->cfg, s, ws->enc_slots);
-  } else if (dtype == MANS_U16) {
-    const uint64_t hdr = adm_u16_header_bytes(n_elems);
-    const uint64_t g = div_up_u64(n_elems, kAdmGroup);
-    if (hdr + n_elems + 32 * g > ws->merged_cap) return MANS_ERR_TOO_LARGE;
-    uint8_t* m = ws->merged + merged_pad(hdr);
-    e = launch_adm_u16_map((const uint16_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
-                           ws->adm_flags, precision, ws->cfg, s);
-    mark(ws, 1, s);
-    if (e == cudaSuccess)
-      e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
-                            ws->ans_flags, precision,
-                            div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s, ws->enc_slots);
-  } else {
-    const uint64_t hdr = adm_u32_header_bytes(n_elems);
-    if (hdr + n_elems > ws->merged_cap) return MANS_ERR_TOO_LARGE;
-    uint8_t* m = ws->merged + merged_pad(hdr);
-    e = launch_adm_u32_map((const uint32_t*)d_in, n_elems, m, ws->merged_cap, ws->ctrl,
-                           ws->adm_flags, precision, ws->cfg, s);
-    mark(ws, 1, s);
-    if (e == cudaSuccess)
-      e = launch_ans_encode(m, (uint8_t*)d_out, out_capacity, osz, nullptr, ws->ctrl,
-                            ws->ans_flags, precision,
-                            div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s, ws->enc_slots);
-  }
-  mark(ws, 2, s);
-  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+  return compress_impl(ws, dtype, MANS_LAYOUT_NATIVE, d_in, n_elems, d_out, out_capacity,
+                       d_out_size, precision, stream, false);
+}
+
+mans_status mans_compress_ex(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                             const void* d_in, uint64_t n_elems, void* d_out,
+                             uint64_t out_capacity, uint64_t* d_out_size, int precision,
+                             mans_stream_t stream) {
+  return compress_impl(ws, dtype, layout, d_in, n_elems, d_out, out_capacity, d_out_size,
+                       precision, stream, false);
+}
+
+mans_status mans_adm_map(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                         const void* d_in, uint64_t n_elems, void* d_out, uint64_t out_capacity,
+                         uint64_t* d_out_size, mans_stream_t stream) {
+  if (dtype == MANS_U8) return MANS_ERR_INVALID_ARG;
+  return compress_impl(ws, dtype, layout, d_in, n_elems, d_out, out_capacity, d_out_size, 10,
+                       stream, true);
 }
 
 mans_status mans_decompress(mans_workspace* ws, mans_dtype dtype, const void* d_in,
                             uint64_t in_size, void* d_out, uint64_t n_elems,
                             mans_stream_t stream) {
-  if (!ws || !d_in || (!d_out && n_elems)) return MANS_ERR_INVALID_ARG;
-  const uint64_t eb = elem_bytes(dtype);
-  if (eb == 0) return MANS_ERR_INVALID_ARG;
-  if (!aligned16(d_in) || (d_out && !aligned16(d_out))) return MANS_ERR_ALIGNMENT;
-  const uint64_t out_bytes = n_elems * eb;
-  if (out_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  cudaError_t e = cudaSuccess;
-  mark(ws, 3, s);
-  if (dtype == MANS_U8) {
-    e = launch_ans_decode((const uint8_t*)d_in, in_size, (uint8_t*)d_out, out_bytes, ws->ctrl, -1,
-                          0, div_up_u64(out_bytes, kAnsBlock), ws->cfg, s);
-    mark(ws, 4, s);
-  } else if (dtype == MANS_U16) {
-    const uint64_t hdr = adm_u16_header_bytes(n_elems);
-    uint8_t* m = ws->merged + merged_pad(hdr);
-    e = launch_ans_decode((const uint8_t*)d_in, in_size, m, ws->merged_cap, ws->ctrl, -1, 1,
-                          div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
-    mark(ws, 4, s);
-    if (e == cudaSuccess)
-      e = launch_adm_u16_unmap(m, n_elems, (uint16_t*)d_out, ws->ctrl, ws->cfg, s);
-  } else {
-    const uint64_t hdr = adm_u32_header_bytes(n_elems);
-    uint8_t* m = ws->merged + merged_pad(hdr);
-    e = launch_ans_decode((const uint8_t*)d_in, in_size, m, ws->merged_cap, ws->ctrl, -1, 1,
-                          div_up_u64(ws->merged_cap, kAnsBlock), ws->cfg, s);
-    mark(ws, 4, s);
-    if (e == cudaSuccess)
-      e = launch_adm_u32_unmap(m, n_elems, (uint32_t*)d_out, ws->ctrl, ws->cfg, s);
-  }
-  mark(ws, 5, s);
-  return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
+  return decompress_impl(ws, dtype, MANS_LAYOUT_NATIVE, d_in, in_size, d_out, n_elems, stream,
+                         false);
+}
+
+mans_status mans_decompress_ex(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                               const void* d_in, uint64_t in_size, void* d_out, uint64_t n_elems,
+                               mans_stream_t stream) {
+  return decompress_impl(ws, dtype, layout, d_in, in_size, d_out, n_elems, stream, false);
+}
+
+mans_status mans_adm_unmap(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                           const void* d_in, uint64_t in_size, void* d_out, uint64_t n_elems,
+                           mans_stream_t stream) {
+  if (dtype == MANS_U8) return MANS_ERR_INVALID_ARG;
+  return decompress_impl(ws, dtype, layout, d_in, in_size, d_out, n_elems, stream, true);
 }
 
 mans_status mans_workspace_set_timing(mans_workspace* ws, int enable) {

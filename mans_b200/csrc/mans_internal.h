@@ -43,11 +43,16 @@ cudaError_t launch_ans_decode(const uint8_t* in, uint64_t in_size, uint8_t* out,
 // ---- ADM uint16 (adm_u16.cu) ----
 // Map n values into the merged buffer M (16-byte aligned codes section),
 // histogram it and normalise (ctrl). flags: >= ceil(n/4096) entries.
+// layout: 0 V15 (canonical), 1 V12, 2 CPU-V2 (see adm_u16.cuh).
 cudaError_t launch_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* m, uint64_t m_cap,
                                Ctrl* ctrl, unsigned long long* flags, int prob_bits,
-                               const LaunchCfg& cfg, cudaStream_t s);
+                               const LaunchCfg& cfg, cudaStream_t s, int layout = 0);
+// V12: v12_excl (>= ceil(n/512) u32) receives the group offsets and
+// scan_flags (>= ceil(n/2^20) + 1 entries) serves the scan's look-back.
 cudaError_t launch_adm_u16_unmap(const uint8_t* m, uint64_t n, uint16_t* out, Ctrl* ctrl,
-                                 const LaunchCfg& cfg, cudaStream_t s);
+                                 const LaunchCfg& cfg, cudaStream_t s, int layout = 0,
+                                 uint32_t* v12_excl = nullptr,
+                                 unsigned long long* scan_flags = nullptr);
 
 // ---- ADM uint32 (adm_u32.cu) ----
 cudaError_t launch_adm_u32_map(const uint32_t* in, uint64_t n, uint8_t* m, uint64_t m_cap,
@@ -59,7 +64,10 @@ cudaError_t launch_adm_u32_unmap(const uint8_t* m, uint64_t n, uint32_t* out, Ct
 // Byte offset of the merged buffer inside its 16-byte aligned region so that
 // the per-element section (codes / records) is 16-byte aligned.
 inline uint64_t merged_pad(uint64_t header_bytes) { return (16 - (header_bytes & 15)) & 15; }
-inline uint64_t adm_u16_header_bytes(uint64_t n) { return 6 * ((n + 511) / 512); }
+inline uint64_t adm_u16_header_bytes(uint64_t n, int layout = 0) {
+  const uint64_t g = (n + 511) / 512;
+  return layout == 1 ? 4 * g : layout == 2 ? 6 * g + 4 : 6 * g;
+}
 inline uint64_t adm_u32_header_bytes(uint64_t n) { return 40 * ((n + 511) / 512); }
 
 }  // namespace mans

@@ -118,9 +118,28 @@ uint64_t mo_adm_u16_merged_size(const uint16_t* in, uint64_t n) {
  * byte holding its end gets its remaining low bits set to 1 (0xFF when the
  * end is byte aligned); later bytes stay 0. mappingcpuV2.cpp:102-114;
  * V15 :345-350. Ragged n (n % 8 != 0) follows the CPU mapping (only valid
- * elements are coded); the reference GPU kernel reads past n there. */
-int64_t mo_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* out, uint64_t cap) {
+ * elements are coded); the reference GPU kernel reads past n there.
+ *
+ * Compatibility layouts (same codes and bits):
+ *   MO_LAYOUT_V12:   [u16 signal length x g][u16 center x g][codes][bits]
+ *                    (mappingV12_bit-adm-thrust-prefixsum.cu :606-634). Its
+ *                    concat kernel (:405-428) copies only lanes that hold an
+ *                    element into a buffer filled with 255 (:504), so a lane
+ *                    past n is 0xFF in all of its len[g] bytes.
+ *   MO_LAYOUT_CPUV2: [i32 signal-length prefix x (g + 1), the last = total]
+ *                    [u16 center x g][codes][bits] (mappingcpuV2.cpp:117-121,
+ *                    271-285). */
+uint64_t mo_adm_u16_header_bytes(uint64_t n, int layout) {
   uint64_t g = div_up(n, ADM_GROUP);
+  if (layout == MO_LAYOUT_V12) return 4 * g;
+  if (layout == MO_LAYOUT_CPUV2) return 6 * g + 4;
+  return 6 * g;
+}
+
+int64_t mo_adm_u16_map_layout(const uint16_t* in, uint64_t n, int layout, uint8_t* out,
+                              uint64_t cap) {
+  uint64_t g = div_up(n, ADM_GROUP);
+  if (layout < 0 || layout > 2) return -2;
   uint32_t* len = (uint32_t*)calloc(g ? g : 1, sizeof(uint32_t));
   uint32_t* ctr = (uint32_t*)calloc(g ? g : 1, sizeof(uint32_t));
   uint64_t tot = 0;
@@ -128,37 +147,49 @@ int64_t mo_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* out, uint64_t ca
     len[grp] = adm_group_len_u16(in, n, grp, &ctr[grp]);
     tot += len[grp];
   }
-  uint64_t msize = 6 * g + n + 32 * tot;
+  const uint64_t hdr = mo_adm_u16_header_bytes(n, layout);
+  uint64_t msize = hdr + n + 32 * tot;
   if (msize > cap) {
     free(len);
     free(ctr);
     return -1;
   }
+  const uint64_t pre = hdr - 2 * g;  /* bytes before the centers */
   uint8_t* p_len = out;
-  uint8_t* p_ctr = out + 4 * g;
-  uint8_t* p_code = out + 6 * g;
-  uint8_t* p_bits = out + 6 * g + n;
+  uint8_t* p_ctr = out + pre;
+  uint8_t* p_code = out + hdr;
+  uint8_t* p_bits = out + hdr + n;
   memset(p_bits, 0, 32 * tot);
   uint64_t excl = 0;
   uint8_t* lanebuf = (uint8_t*)malloc(ADM_U16_MAX_LANE_BYTES + 8);
   for (uint64_t grp = 0; grp < g; ++grp) {
-    wr32(p_len + 4 * grp, (uint32_t)excl);
+    if (layout == MO_LAYOUT_V12) wr16(p_len + 2 * grp, (uint16_t)len[grp]);
+    else wr32(p_len + 4 * grp, (uint32_t)excl);
     wr16(p_ctr + 2 * grp, (uint16_t)ctr[grp]);
     uint32_t L = len[grp];
     for (int l = 0; l < ADM_LANES; ++l) {
       uint64_t s, e;
       lane_range(n, grp, l, &s, &e);
       memset(lanebuf, 0, ADM_U16_MAX_LANE_BYTES + 8);
-      uint32_t b = adm_lane_bits_u16(in, s, e, ctr[grp], lanebuf, p_code + s);
-      if (b < L * 8) lanebuf[b >> 3] |= (uint8_t)(0xFFu >> (b & 7));
+      if (layout == MO_LAYOUT_V12 && s >= e) {
+        memset(lanebuf, 0xFF, L);
+      } else {
+        uint32_t b = adm_lane_bits_u16(in, s, e, ctr[grp], lanebuf, p_code + s);
+        if (b < L * 8) lanebuf[b >> 3] |= (uint8_t)(0xFFu >> (b & 7));
+      }
       memcpy(p_bits + 32 * excl + (uint64_t)l * L, lanebuf, L);
     }
     excl += L;
   }
+  if (layout == MO_LAYOUT_CPUV2) wr32(p_len + 4 * g, (uint32_t)excl);
   free(lanebuf);
   free(len);
   free(ctr);
   return (int64_t)msize;
+}
+
+int64_t mo_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* out, uint64_t cap) {
+  return mo_adm_u16_map_layout(in, n, MO_LAYOUT_V15, out, cap);
 }
 
 /* Inverse mapping. Signal restore follows mappingcpuV2.cpp:161-197 (scan the
@@ -167,19 +198,31 @@ int64_t mo_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* out, uint64_t ca
  * follows :202-224 (odd code: center - diff, even: center + diff, with
  * diff = code/2 + 126*signal). Signal counts are kept as int here; the
  * reference stores them in uint8_t, which wraps for k > 256. */
-int mo_adm_u16_unmap(const uint8_t* m, uint64_t msize, uint64_t n, uint16_t* out) {
+int mo_adm_u16_unmap_layout(const uint8_t* m, uint64_t msize, uint64_t n, int layout,
+                            uint16_t* out) {
   uint64_t g = div_up(n, ADM_GROUP);
-  if (msize < 6 * g + n) return -1;
-  uint64_t bits_bytes = msize - 6 * g - n;
+  if (layout < 0 || layout > 2) return -6;
+  const uint64_t hdr = mo_adm_u16_header_bytes(n, layout);
+  if (msize < hdr + n) return -1;
+  uint64_t bits_bytes = msize - hdr - n;
   if (bits_bytes % 32) return -2;
   uint64_t tot = bits_bytes / 32;
   const uint8_t* p_len = m;
-  const uint8_t* p_ctr = m + 4 * g;
-  const uint8_t* p_code = m + 6 * g;
-  const uint8_t* p_bits = m + 6 * g + n;
+  const uint8_t* p_ctr = m + hdr - 2 * g;
+  const uint8_t* p_code = m + hdr;
+  const uint8_t* p_bits = m + hdr + n;
+  if (layout == MO_LAYOUT_CPUV2 && rd32(p_len + 4 * g) != tot) return -3;
+  uint64_t run = 0;  /* V12: the prefix is recomputed from the lengths */
   for (uint64_t grp = 0; grp < g; ++grp) {
-    uint64_t ex = rd32(p_len + 4 * grp);
-    uint64_t nx = grp + 1 < g ? rd32(p_len + 4 * (grp + 1)) : tot;
+    uint64_t ex, nx;
+    if (layout == MO_LAYOUT_V12) {
+      ex = run;
+      nx = ex + rd16(p_len + 2 * grp);
+      run = nx;
+    } else {
+      ex = rd32(p_len + 4 * grp);
+      nx = grp + 1 < g ? rd32(p_len + 4 * (grp + 1)) : tot;
+    }
     if (nx < ex || nx > tot) return -3;
     uint64_t L = nx - ex;
     uint32_t c = rd16(p_ctr + 2 * grp);
@@ -211,7 +254,12 @@ int mo_adm_u16_unmap(const uint8_t* m, uint64_t msize, uint64_t n, uint16_t* out
       }
     }
   }
+  if (layout == MO_LAYOUT_V12 && run != tot) return -3;
   return 0;
+}
+
+int mo_adm_u16_unmap(const uint8_t* m, uint64_t msize, uint64_t n, uint16_t* out) {
+  return mo_adm_u16_unmap_layout(m, msize, n, MO_LAYOUT_V15, out);
 }
 
 /* ------------------------------------------------------------------------ */

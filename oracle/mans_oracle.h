@@ -26,6 +26,15 @@ uint64_t mo_adm_u16_merged_size(const uint16_t* in, uint64_t n);
 int64_t mo_adm_u16_map(const uint16_t* in, uint64_t n, uint8_t* out, uint64_t cap);
 /* Returns 0 on success, <0 on a malformed merged buffer. */
 int mo_adm_u16_unmap(const uint8_t* m, uint64_t msize, uint64_t n, uint16_t* out);
+/* Compatibility layouts of the uint16 merged buffer (see mans_oracle.c). */
+#define MO_LAYOUT_V15 0
+#define MO_LAYOUT_V12 1
+#define MO_LAYOUT_CPUV2 2
+uint64_t mo_adm_u16_header_bytes(uint64_t n, int layout);
+int64_t mo_adm_u16_map_layout(const uint16_t* in, uint64_t n, int layout, uint8_t* out,
+                              uint64_t cap);
+int mo_adm_u16_unmap_layout(const uint8_t* m, uint64_t msize, uint64_t n, int layout,
+                            uint16_t* out);
 
 /* ---- ADM uint32 (escape-byte format of V9, self-describing merged layout) ---- */
 uint64_t mo_adm_u32_max_merged_size(uint64_t n);

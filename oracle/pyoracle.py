@@ -48,6 +48,9 @@ def lib() -> C.CDLL:
             "mo_adm_u16_merged_size": (u64, [u16p, u64]),
             "mo_adm_u16_map": (i64, [u16p, u64, u8p, u64]),
             "mo_adm_u16_unmap": (i32, [u8p, u64, u64, u16p]),
+            "mo_adm_u16_header_bytes": (u64, [u64, i32]),
+            "mo_adm_u16_map_layout": (i64, [u16p, u64, i32, u8p, u64]),
+            "mo_adm_u16_unmap_layout": (i32, [u8p, u64, u64, i32, u16p]),
             "mo_adm_u32_max_merged_size": (u64, [u64]),
             "mo_adm_u32_map": (i64, [u32p, u64, u8p, u64]),
             "mo_adm_u32_unmap": (i32, [u8p, u64, u64, u32p]),
@@ -79,21 +82,26 @@ def lib() -> C.CDLL:
 
 
 # ---------------------------------------------------------------- ADM u16
-def adm_u16_map(x: np.ndarray) -> np.ndarray:
+# uint16 merged layouts: V15 (canonical), V12 (u16 lengths), CPU-V2 (g + 1 prefix words)
+LAYOUT_V15, LAYOUT_V12, LAYOUT_CPUV2 = 0, 1, 2
+
+
+def adm_u16_map(x: np.ndarray, layout: int = LAYOUT_V15) -> np.ndarray:
     x = np.ascontiguousarray(x, dtype=np.uint16)
     L = lib()
     n = x.size
-    size = L.mo_adm_u16_merged_size(_ptr(x, u16p), n)
+    size = L.mo_adm_u16_merged_size(_ptr(x, u16p), n) - L.mo_adm_u16_header_bytes(n, 0) + \
+        L.mo_adm_u16_header_bytes(n, layout)
     out = np.zeros(max(size, 1), np.uint8)
-    r = L.mo_adm_u16_map(_ptr(x, u16p), n, _ptr(out), size)
+    r = L.mo_adm_u16_map_layout(_ptr(x, u16p), n, layout, _ptr(out), size)
     assert r == size, (r, size)
     return out[:size]
 
 
-def adm_u16_unmap(m: np.ndarray, n: int) -> np.ndarray:
+def adm_u16_unmap(m: np.ndarray, n: int, layout: int = LAYOUT_V15) -> np.ndarray:
     m = np.ascontiguousarray(m, dtype=np.uint8)
     out = np.zeros(max(n, 1), np.uint16)
-    rc = lib().mo_adm_u16_unmap(_ptr(m), m.size, n, _ptr(out, u16p))
+    rc = lib().mo_adm_u16_unmap_layout(_ptr(m), m.size, n, layout, _ptr(out, u16p))
     if rc != 0:
         raise ValueError(f"adm_u16_unmap failed: {rc}")
     return out[:n]
@@ -173,9 +181,9 @@ def ans_mask(s: np.ndarray) -> np.ndarray:
 
 
 # ---------------------------------------------------------------- MANS
-def compress(x: np.ndarray, prob_bits: int = 10) -> np.ndarray:
+def compress(x: np.ndarray, prob_bits: int = 10, layout: int = LAYOUT_V15) -> np.ndarray:
     if x.dtype == np.uint16:
-        m = adm_u16_map(x)
+        m = adm_u16_map(x, layout)
     elif x.dtype == np.uint32:
         m = adm_u32_map(x)
     else:
@@ -183,10 +191,10 @@ def compress(x: np.ndarray, prob_bits: int = 10) -> np.ndarray:
     return ans_encode(m, prob_bits)
 
 
-def decompress(s: np.ndarray, n: int, dtype) -> np.ndarray:
+def decompress(s: np.ndarray, n: int, dtype, layout: int = LAYOUT_V15) -> np.ndarray:
     m = ans_decode(s)
     if np.dtype(dtype) == np.uint16:
-        return adm_u16_unmap(m, n)
+        return adm_u16_unmap(m, n, layout)
     return adm_u32_unmap(m, n)
 
 

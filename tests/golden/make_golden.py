@@ -7,11 +7,15 @@ Runs the reference binaries and libraries built by ``oracle/Makefile`` into
                           (mapping/nv/mappingV15_fused_uint16.cu), file in/out;
 * ``mappingV9``        -- the reference GPU uint32 escape mapping
                           (mapping/nv/mappingV9_fuse.cu), file in/out;
+* ``mappingV12``       -- the reference GPU uint16 mapping with the V12 merged
+                          layout (mapping/nv/mappingV12_bit-adm-thrust-prefixsum.cu),
+                          file in/out;
 * ``ref_ans_driver``   -- the reference GPU rANS codec (include/ans) through
                           ansEncode/ansDecode;
 * ``libref_adm_cpu.so``-- the reference CPU mapping (mapping/cpu/mappingcpuV2.cpp),
                           run with one OpenMP thread (its lane-length update
-                          races when a warp's lanes span OpenMP chunks).
+                          races when a warp's lanes span OpenMP chunks), in
+                          the V15 layout and in its own g + 1 header layout.
 
 Only inputs on which the reference is defined are used: N a multiple of 1024
 (the GPU mappers read and write whole vectors), more than 524,288 uint16
@@ -20,10 +24,15 @@ uninitialised shared variable), lane bit streams under 256 bits (the V15
 lane buffer), uint32 group sums below 2^32, and rANS blocks whose output
 stays under the reference's 5,120-byte block slot.
 
-Usage (from the repository root, on the GPU host):
-    python tests/golden/make_golden.py <outdir>
-Writes ``<outdir>/manifest.json`` and small ``.bin`` files; the committed
-copies live in tests/golden/.
+V12 is run only on N a multiple of 1,024: its decompress kernel writes whole
+1,024-element blocks, past its output buffer for other N.
+
+Usage (from the repository root; the GPU kinds on the GPU host):
+    python tests/golden/make_golden.py <outdir> [--only kind,kind,...]
+    python tests/golden/make_golden.py --merge <outdir>
+The first writes ``<outdir>/manifest.json`` and small ``.bin`` files for the
+selected kinds (all by default); the second merges such a directory into the
+committed copies in tests/golden/.
 """
 from __future__ import annotations
 
@@ -144,12 +153,81 @@ def cpu_cases():
     return out
 
 
-def main(outdir: str) -> None:
+def cpu_native_cases():
+    out = []
+    for i, n in enumerate([1, 16, 511, 512, 513, 1040, 4097, 20000, 70001]):
+        out.append({"name": f"cpuv2native_laplace_{n}", "kind": "adm_u16_cpu_native",
+                    "input": {"gen": "laplace_u16", "n": n, "seed": 400 + i, "b": 300.0}})
+    out.append({"name": "cpuv2native_c1", "kind": "adm_u16_cpu_native",
+                "input": {"gen": "laplace_u16", "n": W.C1_N, "seed": 1}})
+    return out
+
+
+def v12_cases():
+    return [
+        {"name": "v12_laplace_1024", "kind": "adm_u16_v12_gpu",
+         "input": {"gen": "laplace_u16", "n": 1024, "seed": 500, "b": 300.0}},
+        {"name": "v12_laplace_65536", "kind": "adm_u16_v12_gpu",
+         "input": {"gen": "laplace_u16", "n": 65536, "seed": 501, "b": 300.0}},
+        {"name": "v12_gradient", "kind": "adm_u16_v12_gpu",
+         "input": {"gen": "gradient_u16", "n": 1 << 20, "seed": 3}},
+        {"name": "v12_c1", "kind": "adm_u16_v12_gpu",
+         "input": {"gen": "laplace_u16", "n": W.C1_N, "seed": 1}},
+    ]
+
+
+KINDS = ("adm_u16_cpu", "adm_u16_cpu_native", "adm_u16_gpu", "adm_u16_v12_gpu", "adm_u32_gpu", "ans")
+
+
+def merge(src: str) -> None:
+    """Merge the cases of src/manifest.json into the committed golden set."""
+    import shutil
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(src, "manifest.json")) as f:
+        new = json.load(f)
+    path = os.path.join(here, "manifest.json")
+    with open(path) as f:
+        old = json.load(f)
+    names = {c["name"] for c in new}
+    merged = [c for c in old if c["name"] not in names] + new
+    for c in new:
+        for k, v in c.items():
+            if k.endswith("_file"):
+                shutil.copy(os.path.join(src, v), os.path.join(here, v))
+    with open(path, "w") as f:
+        json.dump(merged, f, indent=1)
+    print(f"merged {len(new)} cases; {len(merged)} in total")
+
+
+def main(outdir: str, only=KINDS) -> None:
     os.makedirs(outdir, exist_ok=True)
     manifest = []
     tmp = tempfile.mkdtemp()
+    # --- reference CPU mapping in its own layout (g + 1 prefix words)
+    for c in (cpu_native_cases() if "adm_u16_cpu_native" in only else []):
+        x = gen(c["input"])
+        r = O.RefAdmCpu(x)
+        r.compress()
+        m = r.merged(False)
+        r.decompress()
+        c["ref_roundtrip"] = bool(np.array_equal(r.recovered(), x))
+        record(c, m, outdir, "ref")
+        r.close()
+        manifest.append(c)
+    # --- reference GPU uint16 mapping, V12 layout
+    for c in (v12_cases() if "adm_u16_v12_gpu" in only else []):
+        x = gen(c["input"])
+        assert x.size % 1024 == 0 and max_lane_bits_u16(x) <= 256, c["name"]
+        fi = os.path.join(tmp, "in.u2")
+        fo = os.path.join(tmp, "out.adm")
+        x.tofile(fi)
+        log = run([os.path.join(REF, "mappingV12"), fi, fo, "uint16"])
+        m = np.fromfile(fo, np.uint8)
+        c["ref_log_pass"] = "Pass error check" in log
+        record(c, m, outdir, "ref")
+        manifest.append(c)
     # --- reference CPU mapping (one thread)
-    for c in cpu_cases():
+    for c in (cpu_cases() if "adm_u16_cpu" in only else []):
         x = gen(c["input"])
         r = O.RefAdmCpu(x)
         r.compress()
@@ -164,7 +242,7 @@ def main(outdir: str) -> None:
         r.close()
         manifest.append(c)
     # --- reference GPU uint16 mapping
-    for c in v15_cases():
+    for c in (v15_cases() if "adm_u16_gpu" in only else []):
         x = gen(c["input"])
         assert max_lane_bits_u16(x) <= 256, c["name"]
         fi = os.path.join(tmp, "in.u2")
@@ -176,7 +254,7 @@ def main(outdir: str) -> None:
         record(c, m, outdir, "ref")
         manifest.append(c)
     # --- reference GPU uint32 mapping (records only)
-    for c in v9_cases():
+    for c in (v9_cases() if "adm_u32_gpu" in only else []):
         x = gen(c["input"])
         fi = os.path.join(tmp, "in.u4")
         fo = os.path.join(tmp, "out.adm")
@@ -187,7 +265,7 @@ def main(outdir: str) -> None:
         record(c, m, outdir, "ref")
         manifest.append(c)
     # --- reference GPU rANS
-    for c in ans_cases():
+    for c in (ans_cases() if "ans" in only else []):
         x = gen(c["input"])
         _, bw = O.ans_encode(x, c["prob_bits"], with_block_words=True)
         if bw.size and int(bw.max()) * 2 > 5120 - 16:
@@ -211,4 +289,13 @@ def main(outdir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    args = sys.argv[1:]
+    if args[:1] == ["--merge"]:
+        merge(args[1])
+    else:
+        only = KINDS
+        if "--only" in args:
+            i = args.index("--only")
+            only = tuple(args[i + 1].split(","))
+            args = args[:i] + args[i + 2:]
+        main(args[0] if args else os.path.join(ROOT, "gpurun_out", "golden"), only)

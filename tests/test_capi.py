@@ -80,3 +80,14 @@ def test_division_table_is_exact():
             got = x + np.uint64(bias) + q * np.uint64(cmpl)
             want = (x // np.uint64(pdf)) * np.uint64(M) + x % np.uint64(pdf) + np.uint64(cdf)
             np.testing.assert_array_equal(got, want, err_msg=f"p={p} pdf={pdf}")
+
+
+def test_cli_usage_without_gpu():
+    """The command-line driver (argv of the reference's examples/compress.cu) builds and prints usage."""
+    import subprocess
+
+    from mans_b200 import build as B
+    cli = B.build_cli()
+    r = subprocess.run([cli, "--help"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0
+    assert "<input.img> <temp.ans> <output.img>" in r.stderr

@@ -1,0 +1,104 @@
+"""GPU tests of the on-disk compatibility layouts (mans_compress_ex,
+mans_adm_map / mans_adm_unmap): every mapped byte and stream byte equals the
+oracle's, which is pinned against the reference's V12 and CPU mappers."""
+import numpy as np
+import pytest
+
+import mans_b200 as mb
+from mans_b200 import workloads as W
+from tests.helpers import to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1, 16, 511, 512, 513, 1040, 4097, 70001, 1 << 20]
+
+
+@pytest.fixture(scope="module")
+def ws():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    w = mb.Workspace(64 << 20)
+    yield w
+    w.close()
+
+
+@pytest.mark.parametrize("layout", [mb.LAYOUT_NATIVE, mb.LAYOUT_V12, mb.LAYOUT_CPUV2])
+def test_u16_layouts_match_oracle(ws, oracle, layout):
+    import torch
+    for i, n in enumerate(SIZES):
+        x = (W.gradient_u16, W.laplace_u16, W.volume_u16)[i % 3](n, 600 + i)
+        dx = to_dev(x)
+        m = to_host(mb.adm_map(dx, layout, ws=ws))
+        ref_m = oracle.adm_u16_map(x, layout)
+        np.testing.assert_array_equal(m, ref_m, err_msg=f"map n={n} layout={layout}")
+        back = mb.adm_unmap(to_dev(ref_m), n, torch.uint16, layout, ws=ws)
+        np.testing.assert_array_equal(to_host(back, np.uint16), x, err_msg=f"unmap n={n}")
+        p = 9 + i % 3
+        s = to_host(mb.compress(dx, p, ws=ws, layout=layout))
+        np.testing.assert_array_equal(s, oracle.compress(x, p, layout), err_msg=f"stream n={n}")
+        y = mb.decompress(to_dev(s), n, torch.uint16, ws=ws, layout=layout)
+        np.testing.assert_array_equal(to_host(y, np.uint16), x, err_msg=f"decompress n={n}")
+
+
+def test_u32_native_mapping_matches_oracle(ws, oracle):
+    import torch
+    for i, n in enumerate([1, 511, 513, 70001, 1 << 18]):
+        x = (W.quant_u32, W.detector_u32)[i % 2](n, 700 + i)
+        m = to_host(mb.adm_map(to_dev(x), ws=ws))
+        np.testing.assert_array_equal(m, oracle.adm_u32_map(x))
+        back = mb.adm_unmap(to_dev(m), n, torch.uint32, ws=ws)
+        np.testing.assert_array_equal(to_host(back, np.uint32), x)
+
+
+def test_layout_header_corruption_is_reported(ws, oracle):
+    import torch
+    n = 70001
+    x = W.gradient_u16(n, 5)
+    g = -(-n // 512)
+    m = oracle.adm_u16_map(x, mb.LAYOUT_CPUV2)
+    m[4 * g] ^= 1  # the final prefix word no longer matches the bit section
+    with pytest.raises(mb.MansError) as e:
+        mb.adm_unmap(to_dev(m), n, torch.uint16, mb.LAYOUT_CPUV2, ws=ws)
+    assert e.value.code == 10
+    m = oracle.adm_u16_map(x, mb.LAYOUT_V12)
+    m[0] ^= 1  # group lengths no longer add up to the bit section
+    with pytest.raises(mb.MansError) as e:
+        mb.adm_unmap(to_dev(m), n, torch.uint16, mb.LAYOUT_V12, ws=ws)
+    assert e.value.code == 10
+
+
+def test_layout_argument_checks(ws):
+    import torch
+    x = torch.zeros(1024, dtype=torch.uint32, device="cuda")
+    with pytest.raises(mb.MansError) as e:
+        mb.compress(x, 10, ws=ws, layout=mb.LAYOUT_V12)
+    assert e.value.code == 1
+    with pytest.raises(mb.MansError) as e:
+        mb.adm_map(torch.zeros(16, dtype=torch.uint8, device="cuda"), ws=ws)
+    assert e.value.code == 1
+
+
+@pytest.mark.parametrize("dtype,layout", [("u8", "native"), ("u16", "native"), ("u16", "v12"),
+                                          ("u16", "cpuv2"), ("u32", "native")])
+def test_cli_round_trip(oracle, tmp_path, dtype, layout):
+    """mans_cli <input> <temp> <output>: the temp file is the oracle's stream and
+    the output equals the input, as with the reference's example driver."""
+    import subprocess
+
+    from mans_b200 import build as B
+    cli = B.build_cli()
+    n = 300_001
+    x = {"u8": lambda: W.random_bytes(n, 9, "skewed"), "u16": lambda: W.laplace_u16(n, 9),
+         "u32": lambda: W.detector_u32(n, 9)}[dtype]()
+    fi, ft, fo = tmp_path / "in.img", tmp_path / "t.ans", tmp_path / "out.img"
+    x.tofile(fi)
+    r = subprocess.run([cli, str(fi), str(ft), str(fo), "--dtype", dtype, "--precision", "11",
+                        "--layout", layout], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Compression completed successfully." in r.stdout
+    s = np.fromfile(ft, np.uint8)
+    lay = {"native": 0, "v12": 1, "cpuv2": 2}[layout]
+    ref = oracle.ans_encode(x, 11) if dtype == "u8" else oracle.compress(x, 11, lay)
+    np.testing.assert_array_equal(s, ref)
+    np.testing.assert_array_equal(np.fromfile(fo, x.dtype), x)

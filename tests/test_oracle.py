@@ -94,10 +94,54 @@ def test_golden_ans(case, oracle):
     np.testing.assert_array_equal(oracle.ans_decode(s), x)
 
 
+def _check_layout_case(case, oracle, layout):
+    x = _gen(case["input"], oracle)
+    m = oracle.adm_u16_map(x, layout)
+    assert m.size == case["ref_size"]
+    assert _sha(m) == case["ref_sha256"]
+    if "ref_file" in case:
+        ref = np.fromfile(os.path.join(GOLDEN, case["ref_file"]), np.uint8)
+        np.testing.assert_array_equal(m, ref)
+    np.testing.assert_array_equal(oracle.adm_u16_unmap(m, x.size, layout), x)
+
+
+@pytest.mark.parametrize("case", [c for c in _manifest() if c["kind"] == "adm_u16_cpu_native"],
+                         ids=lambda c: c["name"])
+def test_golden_cpu_native_layout(case, oracle):
+    """Oracle CPU-V2 layout (g + 1 prefix words) == the reference CPU mapping's own merged file."""
+    assert case["ref_roundtrip"]
+    _check_layout_case(case, oracle, oracle.LAYOUT_CPUV2)
+
+
+@pytest.mark.parametrize("case", [c for c in _manifest() if c["kind"] == "adm_u16_v12_gpu"],
+                         ids=lambda c: c["name"])
+def test_golden_v12_layout(case, oracle):
+    """Oracle V12 layout (u16 group lengths) == the reference mappingV12 output file."""
+    assert case.get("ref_log_pass", False)
+    _check_layout_case(case, oracle, oracle.LAYOUT_V12)
+
+
+def test_layouts_round_trip_and_differ_only_in_header(oracle):
+    """All three uint16 layouts round-trip; they share codes and bits except
+    that V12 fills lanes past n with 0xFF."""
+    for n in [16, 512, 1040, 5000, 70001]:
+        x = W.gradient_u16(n, 11)
+        g = -(-n // 512)
+        ms = {lay: oracle.adm_u16_map(x, lay) for lay in (0, 1, 2)}
+        for lay, m in ms.items():
+            np.testing.assert_array_equal(oracle.adm_u16_unmap(m, n, lay), x)
+        body15 = ms[0][6 * g:]
+        np.testing.assert_array_equal(ms[2][6 * g + 4:], body15)
+        np.testing.assert_array_equal(ms[1][4 * g:4 * g + n], body15[:n])  # codes
+        if n % 16 == 0 and n % 512 == 0:
+            np.testing.assert_array_equal(ms[1][4 * g:], body15)
+
+
 def test_golden_manifest_present():
     m = _manifest()
     kinds = {c["kind"] for c in m}
-    assert {"adm_u16_cpu", "adm_u16_gpu", "adm_u32_gpu", "ans"} <= kinds, kinds
+    assert {"adm_u16_cpu", "adm_u16_cpu_native", "adm_u16_gpu", "adm_u16_v12_gpu", "adm_u32_gpu",
+            "ans"} <= kinds, kinds
 
 
 # ---------------------------------------------------------------- live reference CPU mapping
