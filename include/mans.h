@@ -174,6 +174,42 @@ mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_in, uint32_t
                                     uint8_t* d_out, uint32_t* d_out_size, mans_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Self-describing frames: a 64-byte header (magic "MANS", version, element
+ * type, layout, precision, element count, mapped and stream sizes; FORMAT.md
+ * in the repository root documents every byte) in front of a MANS stream, so
+ * a frame decodes with nothing kept out of band. The reference keeps the
+ * element count and type outside the stream (examples/compress.cu:79-97) and,
+ * for uint32, writes no centers or lengths at all (mappingV9_fuse.cu:998);
+ * the frame plus the record layout's header carry both.
+ * ---------------------------------------------------------------------- */
+typedef struct mans_frame_info {
+  mans_dtype dtype;
+  mans_layout layout;
+  int precision;
+  uint32_t header_bytes;   /* 64 */
+  uint64_t n_elems;
+  uint64_t mapped_bytes;   /* ADM output = rANS input */
+  uint64_t stream_bytes;   /* MANS stream after the header */
+} mans_frame_info;
+
+/* Upper bound of a frame's size. */
+uint64_t mans_frame_max_size(mans_dtype dtype, uint64_t n_elems);
+/* Compress into a frame at d_out (16-byte aligned); *d_out_size (device u64)
+ * receives the frame size. */
+mans_status mans_frame_compress(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
+                                const void* d_in, uint64_t n_elems, void* d_out,
+                                uint64_t out_capacity, uint64_t* d_out_size, int precision,
+                                mans_stream_t stream);
+/* Parse and check a frame header held in HOST memory (no GPU needed); avail =
+ * bytes of the frame available (~0 when unknown), checked against its size. */
+mans_status mans_frame_parse(const void* header, uint64_t avail, mans_frame_info* info);
+/* Decompress the frame at d_frame (device) described by info (from
+ * mans_frame_parse) into d_out (out_capacity bytes). */
+mans_status mans_frame_decompress(mans_workspace* ws, const mans_frame_info* info,
+                                  const void* d_frame, void* d_out, uint64_t out_capacity,
+                                  mans_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Batched MANS: many buffers of uneven size and element type in one
  * persistent launch per stage (a device work queue over every buffer's
  * mapping groups and rANS blocks). Each buffer's stream is byte-identical to

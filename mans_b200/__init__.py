@@ -51,6 +51,10 @@ SIGNATURES = {
     "mans_decompress_ex": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp]),
     "mans_adm_map": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp, _vp]),
     "mans_adm_unmap": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp]),
+    "mans_frame_max_size": (_u64, [_i32, _u64]),
+    "mans_frame_compress": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp, _i32, _vp]),
+    "mans_frame_parse": (_i32, [_vp, _u64, _vp]),
+    "mans_frame_decompress": (_i32, [_vp, _vp, _vp, _vp, _u64, _vp]),
     "mans_ans_encode": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
     "mans_ans_decode": (_i32, [_i32, _vp, _vp, _vp]),
     "mans_ans_encode_batch": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
@@ -245,7 +249,8 @@ def adm_unmap(m, n: int, dtype, layout: int = LAYOUT_NATIVE, ws: Optional[Worksp
     own = ws is None
     if own:
         ws = Workspace(max(n * out.element_size(), 1))
-    _check(load().mans_adm_unmap(ws.h, dtype_code(out), layout, m.data_ptr(), m.numel(),
+    _check(load().mans_adm_unmap(ws.h, dtype_code(out), layout, m.data_ptr() if m.numel() else None,
+                                 m.numel(),
                                  out.data_ptr() if n else None, n, _stream_handle(stream)),
            "mans_adm_unmap")
     ws.check(stream, "mans_adm_unmap")
@@ -285,6 +290,70 @@ def decompress(s, n: int, dtype, ws: Optional[Workspace] = None, stream=None,
         ws = Workspace(max(n * out.element_size(), 1))
     decompress_into(ws, s, s.numel(), out, stream, layout)
     ws.check(stream, "mans_decompress")
+    if own:
+        ws.close()
+    return out
+
+
+# ---- self-describing frames ----
+class FrameInfo(C.Structure):
+    """mans_frame_info (include/mans.h)."""
+    _fields_ = [("dtype", C.c_int), ("layout", C.c_int), ("precision", C.c_int),
+                ("header_bytes", C.c_uint32), ("n_elems", C.c_uint64),
+                ("mapped_bytes", C.c_uint64), ("stream_bytes", C.c_uint64)]
+
+
+FRAME_HEADER_BYTES = 64
+_CODE_DTYPE = {MANS_U8: "uint8", MANS_U16: "uint16", MANS_U32: "uint32"}
+
+
+def frame_parse(header: bytes) -> FrameInfo:
+    """Parse a frame header from host bytes (the whole frame, or at least its 64-byte header)."""
+    buf = (C.c_uint8 * max(len(header), 1)).from_buffer_copy(bytes(header) or b"\0")
+    info = FrameInfo()
+    avail = len(header) if len(header) > FRAME_HEADER_BYTES else (1 << 64) - 1
+    _check(load().mans_frame_parse(C.cast(buf, C.c_void_p), avail, C.byref(info)), "mans_frame_parse")
+    return info
+
+
+def frame_compress(x, precision: int = 10, layout: int = LAYOUT_NATIVE,
+                   ws: Optional[Workspace] = None, stream=None):
+    """Compress device tensor x into a self-describing frame (uint8 tensor; synchronises)."""
+    torch = _torch()
+    n = x.numel()
+    code = dtype_code(x)
+    own = ws is None
+    if own:
+        ws = Workspace(max(n * x.element_size(), 1))
+    cap = int(load().mans_frame_max_size(code, n))
+    out = torch.empty(cap, dtype=torch.uint8, device=x.device)
+    size = torch.zeros(1, dtype=torch.int64, device=x.device)
+    _check(load().mans_frame_compress(ws.h, code, layout, x.data_ptr() if n else None, n,
+                                      out.data_ptr(), cap, size.data_ptr(), precision,
+                                      _stream_handle(stream)), "mans_frame_compress")
+    ws.check(stream, "mans_frame_compress")
+    res = out[: int(size.item())].clone()
+    if own:
+        ws.close()
+    return res
+
+
+def frame_decompress(frame, ws: Optional[Workspace] = None, stream=None):
+    """Decompress a frame (device uint8 tensor); the element type and count come from its header."""
+    torch = _torch()
+    info = frame_parse(frame[:FRAME_HEADER_BYTES].cpu().numpy().tobytes())
+    if FRAME_HEADER_BYTES + info.stream_bytes > frame.numel():
+        raise MansError(7, "frame_decompress: truncated frame")
+    dt = getattr(torch, _CODE_DTYPE[info.dtype])
+    out = torch.empty(info.n_elems, dtype=dt, device=frame.device)
+    own = ws is None
+    if own:
+        ws = Workspace(max(out.numel() * out.element_size(), 1))
+    _check(load().mans_frame_decompress(ws.h, C.byref(info), frame.data_ptr(),
+                                        out.data_ptr() if out.numel() else None,
+                                        out.numel() * out.element_size(), _stream_handle(stream)),
+           "mans_frame_decompress")
+    ws.check(stream, "mans_frame_decompress")
     if own:
         ws.close()
     return out

@@ -33,7 +33,18 @@ __global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
     map16_group<kLayout>(in, n, M, m_cap, flags, &ctrl->merged_size, grp, epoch, sink, s_h[warp],
                          lane);
   }
-  hist_merge_and_normalize(s_h, kMapWarps, ctrl, g == 0 ? 0ull : ~0ull, 0, prob_bits);
+  // An empty input maps to nothing, except in the CPU layout, whose g + 1
+  // prefix words are then the single word 0 (mappingcpuV2.cpp:117-121).
+  unsigned long long empty_size = 0;
+  if (kLayout == kLayoutCpuV2 && g == 0) {
+    empty_size = 4;
+    if (blockIdx.x == 0 && t == 0) {
+      reinterpret_cast<uint16_t*>(M)[0] = 0;
+      reinterpret_cast<uint16_t*>(M)[1] = 0;
+      s_h[0][0] += 4;
+    }
+  }
+  hist_merge_and_normalize(s_h, kMapWarps, ctrl, g == 0 ? empty_size : ~0ull, 0, prob_bits);
 }
 
 template <int kLayout>

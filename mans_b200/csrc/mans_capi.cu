@@ -217,10 +217,12 @@ mans_status compress_impl(mans_workspace* ws, mans_dtype dtype, mans_layout layo
 mans_status decompress_impl(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
                             const void* d_in, uint64_t in_size, void* d_out, uint64_t n_elems,
                             mans_stream_t stream, bool unmap_only) {
-  if (!ws || !d_in || (!d_out && n_elems)) return MANS_ERR_INVALID_ARG;
+  // an empty mapped buffer (n = 0) may come without a pointer
+  if (!ws || (!d_in && !(unmap_only && in_size == 0)) || (!d_out && n_elems))
+    return MANS_ERR_INVALID_ARG;
   const uint64_t eb = elem_bytes(dtype);
   if (eb == 0 || !valid_layout(dtype, layout)) return MANS_ERR_INVALID_ARG;
-  if (!aligned16(d_in) || (d_out && !aligned16(d_out))) return MANS_ERR_ALIGNMENT;
+  if ((d_in && !aligned16(d_in)) || (d_out && !aligned16(d_out))) return MANS_ERR_ALIGNMENT;
   const uint64_t out_bytes = n_elems * eb;
   if (out_bytes > ws->max_input_bytes) return MANS_ERR_TOO_LARGE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

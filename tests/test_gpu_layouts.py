@@ -10,7 +10,7 @@ from tests.helpers import to_dev, to_host
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [1, 16, 511, 512, 513, 1040, 4097, 70001, 1 << 20]
+SIZES = [0, 1, 16, 511, 512, 513, 1040, 4097, 70001, 1 << 20]
 
 
 @pytest.fixture(scope="module")
