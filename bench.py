@@ -856,6 +856,17 @@ def serve_trace(srv, reqs, arrivals_s, corpus, streams, check: bool):
         except Exception as e:  # pragma: no cover - reported below
             err.append(e)
 
+    # The check must not allocate: a large allocation that misses torch's
+    # cache calls cudaMalloc / cudaFree, which synchronise the device and
+    # stall the server's scheduler thread along with it.
+    cmp = torch.empty(max(max(int(s.numel()) for s in streams),
+                          max(int(c[0].numel() * c[0].element_size()) for c in corpus)),
+                      dtype=torch.bool, device="cuda") if check else None
+
+    def same(a, b) -> bool:
+        torch.eq(a, b, out=cmp[:a.numel()])
+        return bool(cmp[:a.numel()].all())
+
     th = threading.Thread(target=submitter, daemon=True)
     th.start()
     rec = np.zeros((R, 5), dtype=np.float64)  # latency ns, queued ns, batch items, ok, done time ns
@@ -871,10 +882,10 @@ def serve_trace(srv, reqs, arrivals_s, corpus, streams, check: bool):
             if ok and check:
                 if op == 0:
                     ref = streams[i]
-                    ok = c.out_bytes == ref.numel() and bool(torch.equal(serve.view_device(c.d_out, c.out_bytes), ref))
+                    ok = c.out_bytes == ref.numel() and same(serve.view_device(c.d_out, c.out_bytes), ref)
                 else:
                     x = corpus[i][0].view(torch.uint8)
-                    ok = c.out_bytes == x.numel() and bool(torch.equal(serve.view_device(c.d_out, c.out_bytes), x))
+                    ok = c.out_bytes == x.numel() and same(serve.view_device(c.d_out, c.out_bytes), x)
             if c.status == 0:
                 srv.release(c.ticket)
             bad += 0 if ok else 1
