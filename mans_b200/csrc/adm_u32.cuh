@@ -127,47 +127,49 @@ __device__ __forceinline__ void map32_group(const uint32_t* __restrict__ in, uin
   // publish the group's aggregate now; the prefix is read after staging
   if (lane == 0) st_flag(&flags[grp], make_flag(grp == 0 ? kFlagIncl : kFlagAgg, epoch, gtot));
 
-  // stage the records at phase 0: zero fill, code bytes, escapes, padding
+  // Stage the lane's record at phase 0 as whole 8-byte words: bytes are
+  // appended to a 16-byte accumulator (lo, hi) and each completed word is
+  // stored once; the last word is padded with 255. Record starts are
+  // multiples of 8, so every store is an aligned 8-byte store.
   {
-    uint4* z = reinterpret_cast<uint4*>(stage);
-    const uint32_t chunks = (gtot + 15) >> 4;
-    for (uint32_t i = lane; i < chunks; i += 32) z[i] = make_uint4(0, 0, 0, 0);
-  }
-  __syncwarp();
-  uint8_t* rec = stage + loff;
-  uint32_t pos = 0;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const uint32_t nb = (nbp[i >> 3] >> ((i & 7) * 4)) & 0xfu;
-    const uint32_t code = (codes[i >> 2] >> ((i & 3) * 8)) & 0xffu;
-    if (nb != 0 && !((escm >> i) & 1u)) {
-      rec[pos + nb - 1] = (uint8_t)code;
-      atomicAdd(&hist[code], 1u);
-    }
-    pos += nb;
-  }
-  if (escm) {
-    uint32_t p2 = 0;
+    uint8_t* rec = stage + loff;
+    uint64_t lo = 0, hi = 0;
+    uint32_t fill = 0, wpos = 0;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const uint32_t nb = (nbp[i >> 3] >> ((i & 7) * 4)) & 0xfu;
-      if ((escm >> i) & 1u) {
-        const uint32_t x = __ldg(in + ls + i);  // re-read: keeps v[] out of the live range
-        rec[p2] = 254;
-        rec[p2 + 1] = (uint8_t)(x >> 24);
-        rec[p2 + 2] = (uint8_t)(x >> 16);
-        rec[p2 + 3] = (uint8_t)(x >> 8);
-        rec[p2 + 4] = (uint8_t)x;
-        atomicAdd(&hist[254], 1u);
-        atomicAdd(&hist[x >> 24], 1u);
-        atomicAdd(&hist[(x >> 16) & 0xff], 1u);
-        atomicAdd(&hist[(x >> 8) & 0xff], 1u);
-        atomicAdd(&hist[x & 0xff], 1u);
+      if (nb != 0) {
+        if ((escm >> i) & 1u) {
+          const uint32_t x = __ldg(in + ls + i);  // re-read: keeps v[] out of the live range
+          // 254 then the value big-endian
+          const uint64_t e = 254ull | ((uint64_t)__byte_perm(x, 0, 0x0123) << 8);
+          lo |= e << (8 * fill);
+          hi |= fill ? e >> (64 - 8 * fill) : 0ull;
+          atomicAdd(&hist[254], 1u);
+          atomicAdd(&hist[x >> 24], 1u);
+          atomicAdd(&hist[(x >> 16) & 0xff], 1u);
+          atomicAdd(&hist[(x >> 8) & 0xff], 1u);
+          atomicAdd(&hist[x & 0xff], 1u);
+        } else {
+          // nb - 1 zero bytes, then the code byte
+          const uint32_t code = (codes[i >> 2] >> ((i & 3) * 8)) & 0xffu;
+          const uint32_t at = fill + nb - 1;  // < 15
+          if (at < 8) lo |= (uint64_t)code << (8 * at);
+          else hi |= (uint64_t)code << (8 * (at - 8));
+          atomicAdd(&hist[code], 1u);
+        }
+        fill += nb;
+        if (fill >= 8) {
+          *reinterpret_cast<uint64_t*>(rec + wpos) = lo;
+          wpos += 8;
+          lo = hi;
+          hi = 0;
+          fill -= 8;
+        }
       }
-      p2 += nb;
     }
+    if (fill) *reinterpret_cast<uint64_t*>(rec + wpos) = lo | (~0ull << (8 * fill));
   }
-  for (uint32_t i = rlen; i < padded; ++i) rec[i] = 255;
   {
     // zero bytes: all bytes that are not codes, escapes or padding
     const uint32_t nesc = __popc(escm);
@@ -256,14 +258,17 @@ __device__ __forceinline__ void unmap32_group(const uint8_t* __restrict__ M, uin
   const uint8_t* src = M + rec_base + goff;
   __syncwarp();
   warp_load_phase(stage, src, gtot, lane);
-  // 16 bytes past the staged range may be read by the last window: keep them defined
-  if (lane == 0) {
-    const uint32_t tail = (phase16(src) + gtot + 15) & ~15u;
-    *reinterpret_cast<uint4*>(stage + tail) = make_uint4(0, 0, 0, 0);
-  }
   __syncwarp();
-  // the lane's record, 8-byte aligned in shared memory (phase 0 or 8, loff % 8 == 0)
-  const uint8_t* r = stage + phase16(src) + loff;
+  // The lane's record, 8-byte aligned in shared memory (phase 0 or 8, loff %
+  // 8 == 0), is read as a stream of 8-byte words: A and B hold words blk and
+  // blk + 1, the cursor's bytes are a funnel shift of the two, and a word is
+  // loaded only when the cursor crosses into the next one (at most once per
+  // element, since an element takes at most 8 bytes). Words past the record
+  // read as zeros, so a corrupt record never reads outside it.
+  const uint64_t* rw = reinterpret_cast<const uint64_t*>(stage + phase16(src) + loff);
+  const uint32_t nw = len >> 3;
+  uint64_t A = nw > 0 ? rw[0] : 0ull, B = nw > 1 ? rw[1] : 0ull;
+  uint32_t blk = 0;
   uint32_t vals[16];
   uint32_t cur = 0;
   bool bad = false;
@@ -271,25 +276,29 @@ __device__ __forceinline__ void unmap32_group(const uint8_t* __restrict__ M, uin
   for (int i = 0; i < 16; ++i) {
     vals[i] = 0;
     if (i < cnt) {
-      // bytes cur .. cur+7 from three aligned 32-bit words
-      const uint32_t* wp = reinterpret_cast<const uint32_t*>(r + (cur & ~3u));
-      const uint32_t a = wp[0], b = wp[1], c2 = wp[2];
-      const uint32_t sel = 0x3210u + 0x1111u * (cur & 3u);
-      const uint32_t lo = __byte_perm(a, b, sel), hi = __byte_perm(b, c2, sel);
+      const uint32_t sh = 8u * (cur & 7u);
+      const uint64_t win = sh ? (A >> sh) | (B << (64u - sh)) : A;
+      const uint32_t lo = (uint32_t)win, hi = (uint32_t)(win >> 32);
+      uint32_t used;
       if ((lo & 0xffu) == 254u) {
         vals[i] = __byte_perm(lo, hi, 0x1234);  // big-endian literal, bytes 1..4
-        cur += 5;
+        used = 5;
       } else {
         // leading zero bytes (at most 7), then the code byte
-        // (a window of eight zero bytes only occurs in a corrupt record: z is
-        // clamped so the cursor stays inside the staged record)
+        // (a window of eight zero bytes only occurs in a corrupt record)
         const uint32_t z = min(7u, lo ? (uint32_t)(__ffs(lo) - 1) >> 3
                                       : 4u + ((uint32_t)(__ffs(hi) - 1) >> 3));
-        const uint32_t code = __byte_perm(lo, hi, z) & 0xffu;
-        bad |= (hi == 0 && lo == 0) | (code >= 254u);
+        const uint32_t code = (uint32_t)(win >> (8u * z)) & 0xffu;
+        bad |= (win == 0) | (code >= 254u);
         const uint32_t d = (code >> 1) + 126u * z;
         vals[i] = (code & 1u) ? c - d : c + d;
-        cur += z + 1;
+        used = z + 1;
+      }
+      cur += used;
+      if ((cur >> 3) != blk) {  // crossed into the next word
+        ++blk;
+        A = B;
+        B = blk + 1 < nw ? rw[blk + 1] : 0ull;
       }
     }
   }
