@@ -63,7 +63,7 @@ __global__ __launch_bounds__(kHistThreads) void hist_bytes_kernel(const uint8_t*
 // claimed one at a time (a claim held while another block is encoded would
 // stall every later block's look-back).
 // ------------------------------------------------------------------------
-template <bool kSlots>
+template <bool kSlots, bool kWide>
 __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
     const uint8_t* __restrict__ in, uint8_t* __restrict__ out, uint64_t out_cap,
     unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
@@ -81,8 +81,27 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
   const uint64_t n = __ldcg(&ctrl->merged_size);
   const uint64_t nb = div_up_u64(n, kAnsBlock);
   const uint64_t over = ans_overhead(nb);
+  // Table layout: with a concentrated symbol distribution most lanes of a
+  // step look up the same few entries, and the expanded 16-byte entries save
+  // integer work; with a flat one the lanes spread over many entries, and
+  // the packed 8-byte entries cost fewer shared-memory wavefronts. The
+  // effective number of symbols 2^(2p) / sum(pdf^2) decides (<= 16:
+  // expanded). Both variants are launched; the one that does not match the
+  // table returns at once, before touching any counter. Either layout
+  // yields the same bytes.
+  __shared__ uint32_t s_sq[kEncWarps];
+  {
+    const uint32_t q = ctrl->pdf[t];
+    const uint32_t sq = __reduce_add_sync(0xffffffffu, q * q);
+    if (lane == 0) s_sq[warp] = sq;
+  }
+  __syncthreads();
+  uint64_t tot = 0;
+  for (int w = 0; w < kEncWarps; ++w) tot += s_sq[w];
+  if ((tot * 16ull >= (1ull << (2 * p))) != kWide) return;
   if (!failed) {
-    for (int i = t; i < kAnsSyms; i += kEncThreads) ss.table[i] = ctrl->enc_table[i];
+    if constexpr (kWide) ss.table4[t] = expand_enc_entry(ctrl->enc_table[t], p);
+    else ss.table2[t] = ctrl->enc_table[t];
   }
   __syncthreads();
 
@@ -118,8 +137,12 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
       const uint64_t s1 = ((uint64_t)b + ahead) * kAnsBlock;
       prefetch_l2(in + s1, (uint32_t)min_u64(kAnsBlock, n - s1));
     }
-    encode_block<kSlots>(in, n, out, out_cap, out_size64, out_size32, ctrl->pdf, flags, epoch, p,
-                         sink, ss.table, ss.in[warp], bar, parity, sout, b, lane);
+    if constexpr (kWide)
+      encode_block<kSlots>(in, n, out, out_cap, out_size64, out_size32, ctrl->pdf, flags, epoch,
+                           p, sink, ss.table4, ss.in[warp], bar, parity, sout, b, lane);
+    else
+      encode_block<kSlots>(in, n, out, out_cap, out_size64, out_size32, ctrl->pdf, flags, epoch,
+                           p, sink, ss.table2, ss.in[warp], bar, parity, sout, b, lane);
   }
 
   __syncthreads();
@@ -228,15 +251,22 @@ static int occupancy(const void* fn, int threads, size_t smem) {
 }
 
 void init_ans_launch_cfg(LaunchCfg& cfg) {
-  cudaFuncSetAttribute(ans_encode_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(ans_encode_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(EncSmem));
+  cudaFuncSetAttribute(ans_encode_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(EncSmem));
   cudaFuncSetAttribute(ans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(DecSmem));
-  cfg.enc_ctas = occupancy((const void*)ans_encode_kernel<false>, kEncThreads, sizeof(EncSmem));
-  cudaFuncSetAttribute(ans_encode_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cfg.enc_ctas = max(occupancy((const void*)ans_encode_kernel<false, false>, kEncThreads, sizeof(EncSmem)),
+                     occupancy((const void*)ans_encode_kernel<false, true>, kEncThreads, sizeof(EncSmem)));
+  cudaFuncSetAttribute(ans_encode_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(EncSmemSlots));
-  cfg.enc_slot_ctas = occupancy((const void*)ans_encode_kernel<true>, kEncThreads,
-                                sizeof(EncSmemSlots));
+  cudaFuncSetAttribute(ans_encode_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(EncSmemSlots));
+  cfg.enc_slot_ctas = max(occupancy((const void*)ans_encode_kernel<true, false>, kEncThreads,
+                                    sizeof(EncSmemSlots)),
+                          occupancy((const void*)ans_encode_kernel<true, true>, kEncThreads,
+                                    sizeof(EncSmemSlots)));
   cfg.dec_ctas = occupancy((const void*)ans_decode_kernel, kDecThreads, sizeof(DecSmem));
   cfg.hist_ctas = occupancy((const void*)hist_bytes_kernel, kHistThreads, 0);
 }
@@ -258,16 +288,22 @@ cudaError_t launch_ans_encode(const uint8_t* in, uint8_t* out, uint64_t out_cap,
                               unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
                               unsigned long long* flags, int prob_bits, uint64_t max_blocks,
                               const LaunchCfg& cfg, cudaStream_t s, uint8_t* slots) {
+  // Both table-layout variants are launched; each decides from the pdf on
+  // the device and the one that does not match returns at once.
   const uint64_t want = div_up_u64(max_blocks, kEncWarps);
   if (slots) {
     const uint64_t cap = (uint64_t)cfg.sms * cfg.enc_slot_ctas;
     const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
-    ans_encode_kernel<true><<<grid, kEncThreads, sizeof(EncSmemSlots), s>>>(
+    ans_encode_kernel<true, false><<<grid, kEncThreads, sizeof(EncSmemSlots), s>>>(
+        in, out, out_cap, out_size64, out_size32, ctrl, flags, prob_bits, slots);
+    ans_encode_kernel<true, true><<<grid, kEncThreads, sizeof(EncSmemSlots), s>>>(
         in, out, out_cap, out_size64, out_size32, ctrl, flags, prob_bits, slots);
   } else {
     const uint64_t cap = (uint64_t)cfg.sms * cfg.enc_ctas;
     const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
-    ans_encode_kernel<false><<<grid, kEncThreads, sizeof(EncSmem), s>>>(
+    ans_encode_kernel<false, false><<<grid, kEncThreads, sizeof(EncSmem), s>>>(
+        in, out, out_cap, out_size64, out_size32, ctrl, flags, prob_bits, nullptr);
+    ans_encode_kernel<false, true><<<grid, kEncThreads, sizeof(EncSmem), s>>>(
         in, out, out_cap, out_size64, out_size32, ctrl, flags, prob_bits, nullptr);
   }
   return cudaGetLastError();

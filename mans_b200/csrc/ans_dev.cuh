@@ -19,13 +19,31 @@ constexpr uint32_t kEncSlotBytes = (kEncOutWords * 2 + 127) / 128 * 128;
 
 constexpr uint32_t kEncStageBytes = kAnsBlock + 16;  // a block plus its 16-byte phase
 
+// The encoder's per-symbol entry in shared memory, expanded from the packed
+// table (make_enc_entry) so that a step needs no field extraction:
+// {reciprocal, renormalisation threshold pdf << (31 - p), bias, cmpl | shift << 16}.
+struct EncEntry4 {
+  uint32_t rcp, thr, bias, cs;
+};
+__device__ __forceinline__ EncEntry4 expand_enc_entry(uint2 e, int p) {
+  const uint32_t cmpl = (e.y >> 13) & 0xfffu;
+  return EncEntry4{e.x, ((1u << p) - cmpl) << (kAnsStateBits - p), e.y & 0x1fffu,
+                   cmpl | ((e.y >> 25) << 16)};
+}
+
 struct EncSmemSlots {  // words go to global slots
-  uint2 table[kAnsSyms];
+  union {
+    EncEntry4 table4[kAnsSyms];  // expanded entries
+    uint2 table2[kAnsSyms];      // packed entries
+  };
   alignas(16) uint8_t in[kEncWarps][kEncStageBytes];
   uint64_t bar[kEncWarps];
 };
 struct EncSmem {  // words compacted in shared memory
-  uint2 table[kAnsSyms];
+  union {
+    EncEntry4 table4[kAnsSyms];
+    uint2 table2[kAnsSyms];
+  };
   alignas(16) uint8_t in[kEncWarps][kEncStageBytes];
   uint64_t bar[kEncWarps];
   alignas(16) uint16_t out[kEncWarps][kEncOutWords];
@@ -51,6 +69,24 @@ __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
     x = xr;
   }
 }
+// The same step on an expanded entry (fewer integer operations per symbol).
+__device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
+                                         const EncEntry4* __restrict__ tab,
+                                         uint16_t* __restrict__ out, uint32_t& nw, uint32_t,
+                                         uint32_t, uint32_t ltmask) {
+  const EncEntry4 e = tab[sym];
+  const bool wr = valid && x >= e.thr;
+  const uint32_t vote = __ballot_sync(0xffffffffu, wr);
+  if (wr) out[nw + __popc(vote & ltmask)] = (uint16_t)(x & 0xffffu);
+  nw += __popc(vote);
+  const uint32_t xr = wr ? (x >> 16) : x;
+  if (valid) {
+    const uint32_t q = __umulhi(xr, e.rcp) >> (e.cs >> 16);
+    x = xr + e.bias + q * (e.cs & 0xffffu);
+  } else {
+    x = xr;
+  }
+}
 
 __device__ __forceinline__ void discard_l2_line(const void* p) {
   asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
@@ -63,11 +99,11 @@ __device__ __forceinline__ void discard_l2_line(const void* p) {
 // word buffer -- with kSlots a per-warp slot in global memory, which stays in
 // L2 and is discarded after the final copy (shared memory then holds only
 // the table and the stage), otherwise shared memory.
-template <bool kSlots>
+template <bool kSlots, typename TabT>
 __device__ __forceinline__ void encode_block(
     const uint8_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ out, uint64_t out_cap,
     unsigned long long* out_size64, uint32_t* out_size32, const uint32_t* __restrict__ pdf,
-    unsigned long long* flags, uint32_t epoch, int p, const Sink& sink, const uint2* table,
+    unsigned long long* flags, uint32_t epoch, int p, const Sink& sink, const TabT* table,
     uint8_t* stage, uint64_t* bar, uint32_t& parity, uint16_t* sout, uint32_t b, int lane) {
   const uint32_t ltmask = lanemask_lt();
   const uint32_t mp = 1u << p, sh = kAnsStateBits - p;
