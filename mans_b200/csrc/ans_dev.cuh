@@ -92,23 +92,19 @@ __device__ __forceinline__ void discard_l2_line(const void* p) {
   asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
 }
 
-// Encode block b of one buffer (one warp) and store it at its place in the
-// coalesced stream; the buffer's last block also writes the header and pdf.
-// in / n: the bytes being coded; flags: the buffer's per-block look-back
-// flags; stage / bar / parity: the warp's bulk-copy stage; sout: the warp's
-// word buffer -- with kSlots a per-warp slot in global memory, which stays in
-// L2 and is discarded after the final copy (shared memory then holds only
-// the table and the stage), otherwise shared memory.
-template <bool kSlots, typename TabT>
-__device__ __forceinline__ void encode_block(
-    const uint8_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ out, uint64_t out_cap,
-    unsigned long long* out_size64, uint32_t* out_size32, const uint32_t* __restrict__ pdf,
-    unsigned long long* flags, uint32_t epoch, int p, const Sink& sink, const TabT* table,
-    uint8_t* stage, uint64_t* bar, uint32_t& parity, uint16_t* sout, uint32_t b, int lane) {
+// Encode block b of one buffer (one warp) into the warp's word buffer sout
+// (with kSlots a per-warp slot in global memory, which stays in L2, else
+// shared memory): one bulk copy of the block into the warp's stage, then the
+// interleaved coding with symbols read eight steps ahead; the word count is
+// padded to a 16-byte multiple with zeros (GpuANSEncode.h:275). Returns the
+// number of words; x receives the lane's final state.
+template <typename TabT>
+__device__ __forceinline__ uint32_t encode_words(const uint8_t* __restrict__ in, uint64_t n,
+                                                 uint32_t b, const TabT* table, uint8_t* stage,
+                                                 uint64_t* bar, uint32_t& parity, uint16_t* sout,
+                                                 int p, const Sink& sink, int lane, uint32_t& x) {
   const uint32_t ltmask = lanemask_lt();
   const uint32_t mp = 1u << p, sh = kAnsStateBits - p;
-  const uint64_t nb = div_up_u64(n, kAnsBlock);
-  const uint64_t over = ans_overhead(nb);
   const uint64_t start = (uint64_t)b * kAnsBlock;
   const uint32_t bs = (uint32_t)min_u64(kAnsBlock, n - start);
   // one bulk copy of the block (rounded out to 16-byte boundaries) into this
@@ -123,7 +119,8 @@ __device__ __forceinline__ void encode_block(
   parity ^= 1u;
   const uint8_t* syms = stage + phase16(in + start) + lane;
 
-  uint32_t x = kAnsStartState, nw = 0;
+  x = kAnsStartState;
+  uint32_t nw = 0;
   const uint32_t full = bs >> 5;
   uint32_t j = 0;
   if (full >= 8) {
@@ -148,20 +145,26 @@ __device__ __forceinline__ void encode_block(
     const bool valid = (uint32_t)lane < (bs & 31);
     enc_step(valid, x, valid ? syms[j * 32] : 0u, table, sout, nw, mp, sh, ltmask);
   }
-
-  // Pad the word count to a 16-byte multiple with zeros (GpuANSEncode.h:275).
   const uint32_t padded = (nw + 7) & ~7u;
   if ((uint32_t)lane < padded - nw) sout[nw + lane] = 0;
+  return nw;
+}
 
-  // Single-pass prefix over padded word counts.
-  if (lane == 0) st_flag(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, padded));
-  uint32_t prefix = 0;
-  if (b > 0) {
-    prefix = lookback_exclusive(flags, b, epoch, sink);
-    if (lane == 0) st_flag(&flags[b], make_flag(kFlagIncl, epoch, prefix + padded));
-  }
-  __syncwarp();
-
+// Store block b, whose nw words (padded to padded) start at word `prefix` of
+// the stream's data section: lane states, block word entry, the words, and
+// for the buffer's last block the header, pdf and size. Then the slot's
+// lines are dropped from L2 without write-back.
+template <bool kSlots>
+__device__ __forceinline__ void encode_store(uint8_t* __restrict__ out, uint64_t out_cap,
+                                             uint64_t n, int p, const uint32_t* __restrict__ pdf,
+                                             unsigned long long* out_size64, uint32_t* out_size32,
+                                             const Sink& sink, uint32_t b, uint32_t nw,
+                                             uint32_t prefix, uint32_t x, const uint16_t* sout,
+                                             int lane) {
+  const uint64_t nb = div_up_u64(n, kAnsBlock);
+  const uint64_t over = ans_overhead(nb);
+  const uint32_t bs = (uint32_t)min_u64(kAnsBlock, n - (uint64_t)b * kAnsBlock);
+  const uint32_t padded = (nw + 7) & ~7u;
   const uint64_t end = over + 2ull * ((uint64_t)prefix + padded);
   const bool last = (uint64_t)b + 1 == nb;
   if (last && end > out_cap && lane == 0) report(sink, MANS_ERR_OUTPUT_OVERFLOW, end);
@@ -203,6 +206,27 @@ __device__ __forceinline__ void encode_block(
       discard_l2_line(reinterpret_cast<const uint8_t*>(sout) + 128 * (lane + 32));
     __syncwarp();
   }
+}
+
+// One block as the unit of the single-pass prefix (flags per block).
+template <bool kSlots, typename TabT>
+__device__ __forceinline__ void encode_block(
+    const uint8_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ out, uint64_t out_cap,
+    unsigned long long* out_size64, uint32_t* out_size32, const uint32_t* __restrict__ pdf,
+    unsigned long long* flags, uint32_t epoch, int p, const Sink& sink, const TabT* table,
+    uint8_t* stage, uint64_t* bar, uint32_t& parity, uint16_t* sout, uint32_t b, int lane) {
+  uint32_t x;
+  const uint32_t nw = encode_words(in, n, b, table, stage, bar, parity, sout, p, sink, lane, x);
+  const uint32_t padded = (nw + 7) & ~7u;
+  if (lane == 0) st_flag(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, padded));
+  uint32_t prefix = 0;
+  if (b > 0) {
+    prefix = lookback_exclusive(flags, b, epoch, sink);
+    if (lane == 0) st_flag(&flags[b], make_flag(kFlagIncl, epoch, prefix + padded));
+  }
+  __syncwarp();
+  encode_store<kSlots>(out, out_cap, n, p, pdf, out_size64, out_size32, sink, b, nw, prefix, x,
+                       sout, lane);
 }
 
 constexpr int kDecWarps = 8;
