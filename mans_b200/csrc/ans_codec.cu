@@ -168,7 +168,6 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
 // ------------------------------------------------------------------------
 struct DecSmem {
   uint32_t lut[1 << kMaxProbBits];
-  uint8_t sym[1 << kMaxProbBits];
   alignas(16) uint16_t in[kDecWarps][kEncOutWords];
   uint64_t bar[kDecWarps];
 };
@@ -205,7 +204,7 @@ __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
   __syncthreads();
 
   if (s_ok && n > 0) {
-    const bool tables_ok = build_decode_tables(in, p, sm.lut, sm.sym, s_scan);
+    const bool tables_ok = build_decode_tables(in, p, sm.lut, s_scan);
     if (!tables_ok && t == 0) {
       s_ok = 0;
       if (blockIdx.x == 0) report(sink, MANS_ERR_BAD_STREAM, 1);
@@ -224,7 +223,7 @@ __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
         const uint32_t wn = ((bn.x & 0xffffu) + 7) & ~7u;
         if ((uint64_t)bn.y + wn <= cw) prefetch_l2(in + over + 2ull * bn.y, 2 * wn);
       }
-      decode_block(in, nb, n, cw, p, out, sm.lut, sm.sym, sm.in[warp], bar, parity, sink, b, lane);
+      decode_block(in, nb, n, cw, p, out, sm.lut, sm.in[warp], bar, parity, sink, b, lane);
       b = nxt;
     }
   }

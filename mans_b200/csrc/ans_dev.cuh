@@ -233,13 +233,12 @@ constexpr int kDecWarps = 8;
 constexpr int kDecThreads = kDecWarps * 32;
 constexpr int kMaxProbBits = 11;
 
-// Build the slot tables of a stream's pdf in shared memory (one CTA of 256
-// threads, thread t owns symbol t): lut[s] = pdf << 16 | (s - cdf), sym[s] =
-// the symbol (GpuANSDecode.h:307-377 packs the same fields in one word).
-// Returns false when the pdf does not sum to 2^p.
+// Build the slot table of a stream's pdf in shared memory (one CTA of 256
+// threads, thread t owns symbol t): lut[s] = pdf << 20 | (s - cdf) << 8 |
+// symbol (GpuANSDecode.h:307-377 packs the same fields in one word, in
+// another order). Returns false when the pdf does not sum to 2^p.
 __device__ __forceinline__ bool build_decode_tables(const uint8_t* __restrict__ in, int p,
-                                                    uint32_t* lut, uint8_t* sym,
-                                                    uint32_t* s_scan) {
+                                                    uint32_t* lut, uint32_t* s_scan) {
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const uint16_t* probs = reinterpret_cast<const uint16_t*>(in + kAnsHeaderBytes);
   const uint32_t pdf = __ldg(probs + t);
@@ -260,19 +259,18 @@ __device__ __forceinline__ bool build_decode_tables(const uint8_t* __restrict__ 
   const uint32_t cdf = base + incl - pdf;
   if (total != (1u << p)) return false;
   for (uint32_t j = 0; j < pdf; ++j) {
-    lut[cdf + j] = (pdf << 16) | j;
-    sym[cdf + j] = (uint8_t)t;
+    lut[cdf + j] = (pdf << 20) | (j << 8) | (uint32_t)t;
   }
   return true;
 }
 
 // Decode block b of one stream (one warp) into out + 4096 b. in: the stream
 // (header validated by the caller: nb blocks, n bytes, cw words, precision
-// p); lut / sym: the slot tables; sin / bar / parity: the warp's word stage.
+// p); lut: the slot table; sin / bar / parity: the warp's word stage.
 __device__ __forceinline__ void decode_block(const uint8_t* __restrict__ in, uint32_t nb,
                                              uint32_t n, uint32_t cw, int p,
                                              uint8_t* __restrict__ out, const uint32_t* lut,
-                                             const uint8_t* sym, uint16_t* sin, uint64_t* bar,
+                                             uint16_t* sin, uint64_t* bar,
                                              uint32_t& parity, const Sink& sink, uint32_t b,
                                              int lane) {
   const uint64_t over = ans_overhead(nb);
@@ -308,8 +306,8 @@ __device__ __forceinline__ void decode_block(const uint8_t* __restrict__ in, uin
     if (valid) {
       const uint32_t s0 = x & mask;
       const uint32_t e = lut[s0];
-      dst[j * 32] = sym[s0];
-      x = (e >> 16) * (x >> p) + (e & 0xffffu);
+      dst[j * 32] = (uint8_t)e;
+      x = (e >> 20) * (x >> p) + ((e >> 8) & 0xfffu);
     }
     const bool rd = valid && x < kAnsStartState;
     const uint32_t vote = __ballot_sync(0xffffffffu, rd);
@@ -321,8 +319,8 @@ __device__ __forceinline__ void decode_block(const uint8_t* __restrict__ in, uin
   for (; j >= 0; --j) {
     const uint32_t s0 = x & mask;
     const uint32_t e = lut[s0];
-    dst[j * 32] = sym[s0];
-    x = (e >> 16) * (x >> p) + (e & 0xffffu);
+    dst[j * 32] = (uint8_t)e;
+    x = (e >> 20) * (x >> p) + ((e >> 8) & 0xfffu);
     const bool rd = x < kAnsStartState;
     const uint32_t vote = __ballot_sync(0xffffffffu, rd);
     // A read below the block's first word only happens in a corrupt

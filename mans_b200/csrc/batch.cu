@@ -476,7 +476,6 @@ __global__ __launch_bounds__(32) void batch_plan_decode_kernel(const BatchItem* 
 // ------------------------------------------------------------------------
 struct BatchDecSmem {
   uint32_t lut[1 << kMaxProbBits];
-  uint8_t sym[1 << kMaxProbBits];
   alignas(16) uint16_t in[kBWarps][kEncOutWords];
   uint64_t bar[kBWarps];
 };
@@ -507,7 +506,7 @@ __global__ __launch_bounds__(kBThreads) void batch_decode_kernel(const BatchItem
     BatchState* st = &states[it];
     const uint32_t p = st->p;
     if (it != cur_item) {
-      const bool ok = build_decode_tables(b.in, (int)p, sm.lut, sm.sym, s_scan);
+      const bool ok = build_decode_tables(b.in, (int)p, sm.lut, s_scan);
       if (t == 0) s_tables = ok;
       __syncthreads();
       if (!s_tables && t == 0) report(item_sink(ctrl, st), MANS_ERR_BAD_STREAM, it);
@@ -517,7 +516,7 @@ __global__ __launch_bounds__(kBThreads) void batch_decode_kernel(const BatchItem
     const uint32_t blk = (c - st->unit_base) * kChunkBlocks + warp;
     if (blk < st->nb) {
       uint8_t* dst = b.dtype == MANS_U8 ? b.out : b.m;
-      decode_block(b.in, st->nb, st->n_hdr, st->cw, (int)p, dst, sm.lut, sm.sym, sm.in[warp], bar,
+      decode_block(b.in, st->nb, st->n_hdr, st->cw, (int)p, dst, sm.lut, sm.in[warp], bar,
                    parity, item_sink(ctrl, st), blk, lane);
     }
   }
