@@ -11,7 +11,7 @@ namespace mans {
 // into L2 for whichever warp claims it. The group's bit offset comes from a
 // decoupled look-back over per-group flags.
 template <int kLayout>
-__global__ __launch_bounds__(kMapThreads) void adm_u16_map_kernel(
+__global__ __launch_bounds__(kMapThreads, 6) void adm_u16_map_kernel(
     const uint16_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ M, uint64_t m_cap,
     Ctrl* ctrl, unsigned long long* flags, int prob_bits) {
   __shared__ uint32_t s_h[kMapWarps][kAnsSyms];

@@ -163,7 +163,7 @@ __device__ __forceinline__ void unit_span(const BatchItem& b, uint64_t u, const 
 }
 
 template <uint32_t kDtype>
-__global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 4) void batch_map_kernel(const BatchItem* __restrict__ items,
+__global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_map_kernel(const BatchItem* __restrict__ items,
                                                               BatchState* states, uint32_t count,
                                                               uint64_t total_units, Ctrl* ctrl,
                                                               unsigned long long* flags,
