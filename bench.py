@@ -221,6 +221,15 @@ def ncu_traffic(workload: str) -> dict:
     return out
 
 
+def reduce_max_over_ranks(values, dist=None, device="cuda"):
+    """Max of each value over the ranks (the job's timing is its slowest rank)."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -417,10 +426,7 @@ def run_mans(args):
     comp_ms = k_ms["map"] + k_ms["encode"]
     decomp_ms = k_ms["decode"] + k_ms["unmap"]
 
-    t = torch.tensor([ms_total, comp_ms, decomp_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_total, comp_ms, decomp_ms = [float(v) for v in t.tolist()]
+    ms_total, comp_ms, decomp_ms = reduce_max_over_ranks([ms_total, comp_ms, decomp_ms], dist)
     ms_step = ms_total / args.steps
     value = world * U * args.steps / (ms_total / 1e3) / 1e9
 
@@ -456,10 +462,7 @@ def run_mans(args):
             e2e_ms.append(a.elapsed_time(b))
     ws.check(stream, "e2e")
     e2e_ok = bool(torch.equal(h_out, h_in))
-    te = torch.tensor([sum(e2e_ms) / len(e2e_ms)], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_step_ms = float(te.item())
+    e2e_step_ms = reduce_max_over_ranks([sum(e2e_ms) / len(e2e_ms)], dist)[0]
 
     result = None
     if rank == 0:
@@ -723,10 +726,8 @@ def run_mixed(args):
     stream_equal = stream_equal and bool(torch.equal(outA, outB))
     batch_ok = batch_ok and bool(torch.equal(dec, pool))
 
-    t = torch.tensor([b_c, b_d, plain_c, plain_d, pg_c, pg_d], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    b_c, b_d, plain_c, plain_d, pg_c, pg_d = [float(v) for v in t.tolist()]
+    b_c, b_d, plain_c, plain_d, pg_c, pg_d = reduce_max_over_ranks(
+        [b_c, b_d, plain_c, plain_d, pg_c, pg_d], dist)
     gbs = lambda ms: round(world * U / (ms / 1e3) / 1e9, 3)  # noqa: E731
 
     # ---- end to end through the public API with host buffers (one step)

@@ -347,6 +347,13 @@ uint64_t mans_debug_arena(uint64_t size, const uint64_t* ops, uint32_t n_ops, ui
 /* Library version string. */
 const char* mans_version(void);
 
+/* Diagnostic of the failure path: runs one bounded device wait that nothing
+ * ever satisfies (a look-back over flags no unit publishes) on the current
+ * device and returns the status the kernel recorded -- MANS_ERR_TIMEOUT after
+ * about a second or a few -- and the elapsed time. No fault, trap or hang:
+ * the context stays usable. Allocates and frees its own scratch. */
+mans_status mans_debug_bounded_wait(uint32_t* status, float* elapsed_ms);
+
 /* Diagnostic: the encoder's division-table entry {reciprocal, packed} for a
  * symbol of probability pdf / 2^p and cumulative frequency cdf. */
 void mans_debug_enc_entry(uint32_t pdf, uint32_t cdf, int p, uint32_t out[2]);

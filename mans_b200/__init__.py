@@ -83,6 +83,7 @@ SIGNATURES = {
     "mans_debug_arena": (_u64, [_u64, _vp, _u32, _vp]),
     "mans_version": (C.c_char_p, []),
     "mans_debug_enc_entry": (None, [_u32, _u32, _i32, C.POINTER(_u32)]),
+    "mans_debug_bounded_wait": (_i32, [C.POINTER(_u32), C.POINTER(C.c_float)]),
 }
 
 _LIB: Optional[C.CDLL] = None

@@ -148,6 +148,7 @@ mans_status upload(mans_batch* b, const BatchItem* h, uint32_t count, cudaStream
 
 mans_status run(mans_batch* b, const mans_batch_item* items, uint32_t count, bool compress,
                 cudaStream_t s) {
+  NvtxRange range(compress ? "mans_batch_compress" : "mans_batch_decompress");
   if (!b || (!items && count)) return MANS_ERR_INVALID_ARG;
   if (count > b->max_items) return MANS_ERR_TOO_LARGE;
   if (count == 0) return MANS_OK;

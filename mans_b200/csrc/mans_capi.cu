@@ -146,6 +146,12 @@ __global__ void import_merged_kernel(const uint8_t* __restrict__ src, uint8_t* _
   if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->merged_size = n;
 }
 
+// One warp waits for the prefix of unit 4 over flags that nothing
+// publishes: the bounded wait must run out and record MANS_ERR_TIMEOUT.
+__global__ void debug_wait_kernel(unsigned long long* flags, Ctrl* ctrl) {
+  lookback_exclusive(flags, 4, 1u, sink_of(ctrl));
+}
+
 unsigned copy_grid(const LaunchCfg& cfg, uint64_t n) {
   const uint64_t want = div_up_u64(n, 256 * 16);
   const uint64_t cap = (uint64_t)cfg.sms * 8;
@@ -161,6 +167,7 @@ mans_status compress_impl(mans_workspace* ws, mans_dtype dtype, mans_layout layo
                           const void* d_in, uint64_t n_elems, void* d_out, uint64_t out_capacity,
                           uint64_t* d_out_size, int precision, mans_stream_t stream,
                           bool map_only) {
+  NvtxRange range(map_only ? "mans_adm_map" : "mans_compress");
   if (!ws || !d_out || !d_out_size || (!d_in && n_elems)) return MANS_ERR_INVALID_ARG;
   const uint64_t eb = elem_bytes(dtype);
   if (eb == 0 || !valid_layout(dtype, layout)) return MANS_ERR_INVALID_ARG;
@@ -217,6 +224,7 @@ mans_status compress_impl(mans_workspace* ws, mans_dtype dtype, mans_layout layo
 mans_status decompress_impl(mans_workspace* ws, mans_dtype dtype, mans_layout layout,
                             const void* d_in, uint64_t in_size, void* d_out, uint64_t n_elems,
                             mans_stream_t stream, bool unmap_only) {
+  NvtxRange range(unmap_only ? "mans_adm_unmap" : "mans_decompress");
   // an empty mapped buffer (n = 0) may come without a pointer
   if (!ws || (!d_in && !(unmap_only && in_size == 0)) || (!d_out && n_elems))
     return MANS_ERR_INVALID_ARG;
@@ -555,6 +563,41 @@ mans_status mans_ans_last_status(mans_stream_t stream, uint64_t* detail) {
 }
 
 // Diagnostic: the encoder's division table entry for (pdf, cdf, p).
+mans_status mans_debug_bounded_wait(uint32_t* status, float* elapsed_ms) {
+  NvtxRange range("mans_debug_bounded_wait");
+  if (!status) return MANS_ERR_INVALID_ARG;
+  uint8_t* mem = nullptr;
+  const size_t flags_off = (sizeof(Ctrl) + 255) / 256 * 256;
+  const size_t bytes = flags_off + 64 * sizeof(unsigned long long);
+  if (cudaMalloc(&mem, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return MANS_ERR_OUT_OF_MEMORY;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaError_t e = cudaMemset(mem, 0, bytes);
+  Ctrl* ctrl = reinterpret_cast<Ctrl*>(mem);
+  cudaEventRecord(e0, 0);
+  if (e == cudaSuccess) {
+    debug_wait_kernel<<<1, 32>>>(reinterpret_cast<unsigned long long*>(mem + flags_off), ctrl);
+    e = cudaGetLastError();
+  }
+  cudaEventRecord(e1, 0);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  uint32_t st = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&st, &ctrl->status, sizeof(st), cudaMemcpyDeviceToHost);
+  float ms = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(mem);
+  if (e != cudaSuccess) return MANS_ERR_CUDA;
+  *status = st;
+  if (elapsed_ms) *elapsed_ms = ms;
+  return MANS_OK;
+}
+
 void mans_debug_enc_entry(uint32_t pdf, uint32_t cdf, int p, uint32_t out[2]) {
   const uint2 e = make_enc_entry(pdf, cdf, p);
   out[0] = e.x;

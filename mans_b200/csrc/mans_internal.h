@@ -5,9 +5,20 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace mans {
 
 struct Ctrl;
+
+// NVTX range over a host call (free when no tool is attached), so a trace
+// shows each codec call beside the kernels it enqueued.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct LaunchCfg {
   int sms = 148;        // multiprocessors of the device

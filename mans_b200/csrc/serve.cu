@@ -195,6 +195,8 @@ bool admit(mans_server* s, Lane& L) {
 void fail_all(mans_server* s, Lane& L, mans_status st);
 
 void launch(mans_server* s, Lane& L) {
+  NvtxRange range(L.op == MANS_OP_COMPRESS ? "mans_server_launch_compress"
+                                           : "mans_server_launch_decompress");
   const uint32_t n = (uint32_t)L.reqs.size();
   const uint64_t t = now_ns();
   for (auto& r : L.reqs) r.t_launch = t;
