@@ -203,3 +203,39 @@ def test_repeated_calls_identical(ws):
     a = gpu_compress(ws, x, 10)
     b = gpu_compress(ws, x, 10)
     np.testing.assert_array_equal(a, b)
+
+
+def test_single_path_cuda_graph_replay(ws, oracle):
+    """mans_compress / mans_decompress captured in a CUDA graph and replayed
+    with new input: every stream and value matches (the look-back epoch and
+    all bounds live on the device)."""
+    import torch
+    n = 300_001
+    x0 = W.laplace_u16(n, 41)
+    dx = to_dev(x0)
+    cap = mb.max_compressed_size(2, n)
+    out = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    size = torch.zeros(1, dtype=torch.int64, device="cuda")
+    back = torch.empty(n, dtype=torch.uint16, device="cuda")
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        mb.compress_into(ws, dx, out, size, 10, s)
+        mb.decompress_into(ws, out, cap, back, s)
+    torch.cuda.synchronize()
+    ws.check(what="warm-up")
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        mb.compress_into(ws, dx, out, size, 10, s)
+        mb.decompress_into(ws, out, cap, back, s)
+    torch.cuda.synchronize()
+    for rep in range(3):
+        x = (W.laplace_u16, W.gradient_u16, W.volume_u16)[rep](n, 50 + rep)
+        dx.copy_(to_dev(x))
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        ws.check(what=f"replay {rep}")
+        np.testing.assert_array_equal(to_host(out[: int(size.item())]), oracle.compress(x, 10))
+        np.testing.assert_array_equal(to_host(back, np.uint16), x)
+    del g
