@@ -442,7 +442,7 @@ def run_mans(args):
     scap = C + 4096
     e2e_seq_ms = []
     sets = []
-    depth = 2  # buffer sets in flight
+    depth = int(os.environ.get("MANS_E2E_DEPTH", "2"))  # buffer sets in flight
     for i in range(depth):
         wsi = ws if i == 0 else mb.Workspace(U)
         sets.append({
@@ -503,7 +503,7 @@ def run_mans(args):
             S = sets[k % depth]
             first_half(S)
             pending.append(S)
-            if len(pending) == depth - 1 or k == steps_here - 1:
+            if len(pending) == depth:  # the oldest step's second half
                 second_half(pending.pop(0))
         while pending:
             second_half(pending.pop(0))
