@@ -239,3 +239,53 @@ def test_single_path_cuda_graph_replay(ws, oracle):
         np.testing.assert_array_equal(to_host(out[: int(size.item())]), oracle.compress(x, 10))
         np.testing.assert_array_equal(to_host(back, np.uint16), x)
     del g
+
+
+# ---------------------------------------------------------------- maximum sizes
+def _free_gib():
+    import torch
+    free, _ = torch.cuda.mem_get_info()
+    return free / (1 << 30)
+
+
+def test_max_size_u32_round_trip(torch_cuda):
+    """2^30 uint32 values (4 GiB; the reference's uint32 mapper is limited to
+    2^27 per call): bit-exact round trip and a stream that the decoder
+    accepts; the mapped size stays below the 32-bit stream field."""
+    import torch
+
+    import bench
+    if _free_gib() < 40:
+        pytest.skip("needs ~40 GiB free")
+    n = 1 << 30
+    x = bench.gen_device("detector_u32", n, 12)
+    w = mb.Workspace(n * 4)
+    try:
+        s = mb.compress(x, 10, ws=w)
+        hdr = to_host(s[:32]).view(np.uint32)
+        assert hdr[0] == 0xD00D0001 and hdr[2] < (1 << 32) - 16
+        y = mb.decompress(s, n, torch.uint32, ws=w)
+        assert torch.equal(y, x)
+    finally:
+        w.close()
+
+
+def test_max_size_u8_round_trip(torch_cuda):
+    """4.0e9 raw bytes, just below the stream's 32-bit byte count."""
+    import torch
+    if _free_gib() < 30:
+        pytest.skip("needs ~30 GiB free")
+    n = 4_000_000_000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    x = (torch.randint(0, 16, (n,), device="cuda", dtype=torch.uint8, generator=g) *
+         torch.randint(0, 2, (n,), device="cuda", dtype=torch.uint8, generator=g))
+    w = mb.Workspace(n)
+    try:
+        s = mb.compress(x, 11, ws=w)
+        hdr = to_host(s[:32]).view(np.uint32)
+        assert int(hdr[2]) == n and int(hdr[1]) == -(-n // 4096)
+        y = mb.decompress(s, n, torch.uint8, ws=w)
+        assert torch.equal(y, x)
+    finally:
+        w.close()
