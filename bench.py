@@ -238,18 +238,36 @@ def dist_env():
 
 
 # ---------------------------------------------------------------- CPU timing (reference arm / baseline)
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_round_trip(workload: str, n: int, reps: int, warm: int, seed: int = 7) -> dict:
-    """Round trip of a host sample through the CPU path on all host cores."""
-    return cpu_round_trip_array(gen_host_sample(workload, n, seed), reps, warm,
-                                f"the same generator, seed {seed}")
+    """Round trip of a host sample through the CPU path on all host cores,
+    plus a one-thread figure on a sixteenth of the sample."""
+    x = gen_host_sample(workload, n, seed)
+    r = cpu_round_trip_array(x, reps, warm, f"the same generator, seed {seed}")
+    x1 = x[: max(1, (x.size // 16) // 512 * 512)]
+    r1 = cpu_round_trip_array(x1, 1, 1, f"the same generator, seed {seed}", threads=1)
+    r["one_thread"] = {"value": r1["value"], "unit": r1["unit"], "sample": r1["sample"]}
+    return r
 
 
-def cpu_round_trip_array(x: np.ndarray, reps: int, warm: int, what: str) -> dict:
+def cpu_round_trip_array(x: np.ndarray, reps: int, warm: int, what: str,
+                         threads: int = 0) -> dict:
     from oracle import pyoracle as O
     n = x.size
     L = O.lib()
     u8p, u16p, u32p = O.u8p, O.u16p, O.u32p
-    cores = os.cpu_count() or 1
+    cores = threads or os.cpu_count() or 1
+    L.mo_set_threads(cores)
     times = []
     kind = "port"
     detail = ""
@@ -318,6 +336,7 @@ def cpu_round_trip_array(x: np.ndarray, reps: int, warm: int, what: str) -> dict
     mean = sum(times) / len(times)
     nbytes = n * x.itemsize
     return {"value": round(nbytes / mean / 1e9, 4), "unit": "GB/s", "cores": cores, "kind": kind,
+            "cpu_model": cpu_model(),
             "sample": f"{n} elements ({nbytes / 1e6:.1f} MB) of {what}; "
                       f"mean of {reps} round trips after {warm} warm-ups; {detail}",
             "round_trip_ok": ok, "ms_per_round_trip": round(mean * 1e3, 3)}

@@ -751,6 +751,14 @@ int mo_mans_decompress_u32(const uint8_t* in, uint64_t in_size, uint64_t n, uint
 #include <omp.h>
 #endif
 
+void mo_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n > 0 ? n : 1);
+#else
+  (void)n;
+#endif
+}
+
 void mo_ans_histogram_par(const uint8_t* in, uint64_t n, uint32_t hist[256]) {
   memset(hist, 0, 256 * sizeof(uint32_t));
 #pragma omp parallel

@@ -71,6 +71,7 @@ int64_t mo_mans_compress_u32(int prob_bits, const uint32_t* in, uint64_t n, uint
 int mo_mans_decompress_u32(const uint8_t* in, uint64_t in_size, uint64_t n, uint32_t* out);
 
 /* ---- OpenMP variants (same bytes), used as the timed CPU baseline ---- */
+void mo_set_threads(int n); /* threads of the variants below */
 void mo_ans_histogram_par(const uint8_t* in, uint64_t n, uint32_t hist[256]);
 uint64_t mo_ans_par_scratch_words(uint64_t n);
 int64_t mo_ans_encode_par(int prob_bits, const uint8_t* in, uint64_t n, uint8_t* out,

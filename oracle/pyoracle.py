@@ -66,6 +66,7 @@ def lib() -> C.CDLL:
             "mo_mans_decompress_u16": (i32, [u8p, u64, u64, u16p]),
             "mo_mans_compress_u32": (i64, [i32, u32p, u64, u8p, u64]),
             "mo_mans_decompress_u32": (i32, [u8p, u64, u64, u32p]),
+            "mo_set_threads": (None, [i32]),
             "mo_ans_histogram_par": (None, [u8p, u64, u32p]),
             "mo_ans_par_scratch_words": (u64, [u64]),
             "mo_ans_encode_par": (i64, [i32, u8p, u64, u8p, u64, u16p, u32p, u32p]),
