@@ -8,7 +8,6 @@ test calls it through the C ABI twice in a row and checks each stream
 against the existing entry point's (mans_ans_encode), byte for byte. This
 file is collected last so that a failure here stops a run only after every
 other test has run."""
-import ctypes as C
 
 import numpy as np
 import pytest
