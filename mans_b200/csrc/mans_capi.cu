@@ -3,6 +3,7 @@
 // rANS entry points.
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <utility>
@@ -462,16 +463,30 @@ mans_status mans_workspace_kernel_times(mans_workspace* ws, float ms[4], int cal
 // allocates only when the workspace has to grow.
 // ------------------------------------------------------------------------
 namespace {
+// A workspace replaced by a larger one is destroyed when its last user
+// drops it, after the work queued on its stream has finished, so a call on
+// another host thread that still holds it never sees its memory freed.
+struct WsRelease {
+  cudaStream_t s;
+  void operator()(mans_workspace* ws) const {
+    cudaStreamSynchronize(s);
+    mans_workspace_destroy(ws);
+  }
+};
+using WsRef = std::shared_ptr<mans_workspace>;
 std::mutex g_mu;
-std::map<std::pair<int, cudaStream_t>, mans_workspace*> g_ws;
+std::map<std::pair<int, cudaStream_t>, WsRef> g_ws;
 
-mans_workspace* default_ws(cudaStream_t s, uint64_t need_bytes, mans_status* st) {
+// The caller holds g_mu until its launches are enqueued: the calls of
+// several host threads on one stream share that stream's workspace, so one
+// call's launches (histogram, then encode) must stay adjacent in stream
+// order.
+WsRef default_ws(cudaStream_t s, uint64_t need_bytes, mans_status* st) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     *st = MANS_ERR_CUDA;
     return nullptr;
   }
-  std::lock_guard<std::mutex> lock(g_mu);
   auto key = std::make_pair(dev, s);
   auto it = g_ws.find(key);
   if (it != g_ws.end() && it->second->max_input_bytes >= need_bytes) {
@@ -481,16 +496,15 @@ mans_workspace* default_ws(cudaStream_t s, uint64_t need_bytes, mans_status* st)
   uint64_t cap = 1ull << 20;
   if (it != g_ws.end()) {
     cap = it->second->max_input_bytes * 2;
-    cudaStreamSynchronize(s);
-    mans_workspace_destroy(it->second);
     g_ws.erase(it);
   }
   while (cap < need_bytes) cap *= 2;
   mans_workspace* ws = nullptr;
   *st = mans_workspace_create(&ws, cap, 0);
   if (*st != MANS_OK) return nullptr;
-  g_ws[key] = ws;
-  return ws;
+  WsRef ref(ws, WsRelease{s});
+  g_ws[key] = ref;
+  return ref;
 }
 }  // namespace
 
@@ -508,7 +522,8 @@ mans_status mans_ans_encode(int precision, const uint8_t* d_in, uint32_t in_size
   if ((d_in && !aligned16(d_in)) || !aligned16(d_out)) return MANS_ERR_ALIGNMENT;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   mans_status st = MANS_OK;
-  mans_workspace* ws = default_ws(s, in_size, &st);
+  std::lock_guard<std::mutex> lock(g_mu);
+  const WsRef ws = default_ws(s, in_size, &st);
   if (!ws) return st;
   cudaError_t e = launch_hist_bytes(d_in, in_size, ws->ctrl, precision, ws->cfg, s);
   if (e == cudaSuccess)
@@ -525,7 +540,8 @@ mans_status mans_ans_decode(int precision, const uint8_t* d_in, uint8_t* d_out,
   if (!aligned16(d_in) || !aligned16(d_out)) return MANS_ERR_ALIGNMENT;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   mans_status st = MANS_OK;
-  mans_workspace* ws = default_ws(s, 0, &st);
+  std::lock_guard<std::mutex> lock(g_mu);
+  const WsRef ws = default_ws(s, 0, &st);
   if (!ws) return st;
   // Sizes come from the stream header on the device (as in the reference):
   // the grid is one resident wave and the caller sized d_out from the header.
@@ -549,7 +565,7 @@ mans_status mans_ans_last_status(mans_stream_t stream, uint64_t* detail) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return MANS_ERR_CUDA;
-  mans_workspace* ws = nullptr;
+  WsRef ws;
   {
     std::lock_guard<std::mutex> lock(g_mu);
     auto it = g_ws.find(std::make_pair(dev, s));
@@ -559,7 +575,7 @@ mans_status mans_ans_last_status(mans_stream_t stream, uint64_t* detail) {
     }
     ws = it->second;
   }
-  return mans_workspace_status(ws, stream, detail);
+  return mans_workspace_status(ws.get(), stream, detail);
 }
 
 // Diagnostic: the encoder's division table entry for (pdf, cdf, p).
