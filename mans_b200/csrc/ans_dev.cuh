@@ -51,6 +51,8 @@ struct EncSmem {  // words compacted in shared memory
 
 // One interleaved step: renormalise (emit 16 bits, lanes in ascending order
 // into the compacted word buffer), then x = (x/pdf << p) + x%pdf + cdf.
+// kGuard: drop words past the buffer (see encode_words).
+template <bool kGuard = false>
 __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
                                          const uint2* __restrict__ tab, uint16_t* __restrict__ out,
                                          uint32_t& nw, uint32_t mp, uint32_t sh, uint32_t ltmask) {
@@ -59,7 +61,10 @@ __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
   const uint32_t thr = (mp - cmpl) << sh;
   const bool wr = valid && x >= thr;
   const uint32_t vote = __ballot_sync(0xffffffffu, wr);
-  if (wr) out[nw + __popc(vote & ltmask)] = (uint16_t)(x & 0xffffu);
+  if (wr) {
+    const uint32_t idx = nw + __popc(vote & ltmask);
+    if (!kGuard || idx < kEncOutWords) out[idx] = (uint16_t)(x & 0xffffu);
+  }
   nw += __popc(vote);
   const uint32_t xr = wr ? (x >> 16) : x;
   if (valid) {
@@ -70,6 +75,7 @@ __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
   }
 }
 // The same step on an expanded entry (fewer integer operations per symbol).
+template <bool kGuard = false>
 __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
                                          const EncEntry4* __restrict__ tab,
                                          uint16_t* __restrict__ out, uint32_t& nw, uint32_t,
@@ -77,7 +83,10 @@ __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
   const EncEntry4 e = tab[sym];
   const bool wr = valid && x >= e.thr;
   const uint32_t vote = __ballot_sync(0xffffffffu, wr);
-  if (wr) out[nw + __popc(vote & ltmask)] = (uint16_t)(x & 0xffffu);
+  if (wr) {
+    const uint32_t idx = nw + __popc(vote & ltmask);
+    if (!kGuard || idx < kEncOutWords) out[idx] = (uint16_t)(x & 0xffffu);
+  }
   nw += __popc(vote);
   const uint32_t xr = wr ? (x >> 16) : x;
   if (valid) {
@@ -123,11 +132,14 @@ __device__ __forceinline__ uint32_t encode_words(const uint8_t* __restrict__ in,
   uint32_t nw = 0;
   const uint32_t full = bs >> 5;
   uint32_t j = 0;
+  // Each step adds at most 32 words, and nw is the same in every lane: while
+  // nw <= kRoom the next eight steps fit in the buffer without a check.
+  constexpr uint32_t kRoom = kEncOutWords - 8 * 32;
   if (full >= 8) {
     uint32_t cur[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) cur[u] = syms[u * 32];
-    for (; j + 16 <= full; j += 8) {
+    for (; j + 16 <= full && nw <= kRoom; j += 8) {
       uint32_t nx[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) nx[u] = syms[(j + 8 + u) * 32];
@@ -136,14 +148,31 @@ __device__ __forceinline__ uint32_t encode_words(const uint8_t* __restrict__ in,
 #pragma unroll
       for (int u = 0; u < 8; ++u) cur[u] = nx[u];
     }
+    if (nw <= kRoom) {
 #pragma unroll
-    for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
-    j += 8;
+      for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
+      j += 8;
+    }
   }
-  for (; j < full; ++j) enc_step(true, x, syms[j * 32], table, sout, nw, mp, sh, ltmask);
-  if (bs & 31) {
-    const bool valid = (uint32_t)lane < (bs & 31);
-    enc_step(valid, x, valid ? syms[j * 32] : 0u, table, sout, nw, mp, sh, ltmask);
+  const bool tail_valid = (uint32_t)lane < (bs & 31);
+  if (nw <= kRoom && full - j <= 7) {  // at most eight more steps
+    for (; j < full; ++j) enc_step(true, x, syms[j * 32], table, sout, nw, mp, sh, ltmask);
+    if (bs & 31)
+      enc_step(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw, mp, sh, ltmask);
+  } else {
+    for (; j < full; ++j)
+      enc_step<true>(true, x, syms[j * 32], table, sout, nw, mp, sh, ltmask);
+    if (bs & 31)
+      enc_step<true>(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw, mp, sh,
+                     ltmask);
+  }
+  // A table that fits the block's bytes keeps each lane within its bound of
+  // words (kAnsMaxBlockWords / 32); only a table built from other bytes (two
+  // calls racing on one scratch area) can exceed it. Word writes past the
+  // buffer are dropped above, and the block is reported.
+  if (nw > kAnsMaxBlockWords) {
+    if (lane == 0) report(sink, MANS_ERR_CORRUPT, b);
+    nw = kAnsMaxBlockWords;
   }
   const uint32_t padded = (nw + 7) & ~7u;
   if ((uint32_t)lane < padded - nw) sout[nw + lane] = 0;

@@ -62,6 +62,22 @@ def test_ans_bytes_parity(ws, oracle, p, kind):
         np.testing.assert_array_equal(gpu_decompress(ws, s, n, np.uint8), x)
 
 
+def test_ans_blocks_near_the_word_bound(ws, oracle):
+    """Blocks of rare symbols at p = 11: each symbol has frequency 1 and costs
+    11 bits, so a block takes about 2,816 words -- past the point where the
+    encoder checks its word buffer step by step. Streams stay bit-exact."""
+    n = 1 << 20
+    x = np.zeros(n, np.uint8)
+    for blk in (3, 100, 255):  # whole 4 KiB blocks of symbols 1..255
+        x[blk * 4096:(blk + 1) * 4096] = 1 + np.arange(4096) % 255
+    ref, bw = oracle.ans_encode(x, 11, with_block_words=True)
+    assert int(bw.max()) > 2632  # the guarded tail runs
+    s = gpu_compress(ws, x, 11)
+    np.testing.assert_array_equal(s, ref)
+    y = mb.decompress(to_dev(s), n, __import__("torch").uint8, ws=ws)
+    np.testing.assert_array_equal(to_host(y), x)
+
+
 def test_ans_decode_of_oracle_stream(ws, oracle):
     x = W.random_bytes(300_000, 5, "skewed")
     s = oracle.ans_encode(x, 11)
