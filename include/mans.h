@@ -139,7 +139,10 @@ mans_status mans_adm_unmap(mans_workspace* ws, mans_dtype dtype, mans_layout lay
  * arguments and meaning as the reference; they run on a library-owned
  * workspace per (device, stream) that is created on first use, so the first
  * call on a stream allocates. Errors the reference could only print are
- * returned as a status.
+ * returned as a status. They may be called from several host threads, on one
+ * stream or on several: each call enqueues its launches under a lock, so the
+ * launches of one call stay adjacent in stream order, and a workspace that
+ * grows is freed only after the work queued on it has finished.
  * ---------------------------------------------------------------------- */
 /* multibyte_ans::ansEncode, include/ans/GpuANSEncode.h:286. d_out must hold
  * mans_ans_max_compressed_size(in_size) bytes; *d_out_size is a device u32. */
