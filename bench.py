@@ -780,6 +780,7 @@ def run_mixed(args):
     batch_ok = bool(torch.equal(dec, pool))
     tuned_ms = batch.autotune(items_c, stream) if not args.no_autotune else None
     sched, sched_max = batch.schedule()
+    sched_full, _ = batch.schedule_ex()
     batch.set_timing(True)
     for _ in range(3):
         batch.compress_async(items_c)
@@ -870,6 +871,7 @@ def run_mixed(args):
                         "round_trip_gbs": gbs(b_c + b_d), "ms_compress": round(b_c, 3),
                         "ms_decompress": round(b_d, 3), "graph": True,
                         "schedule_ctas_per_sm": sched, "schedule_max": sched_max,
+                        "schedule": sched_full,
                         "autotune_best_ms": tuned_ms,
                         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()}},
             "plain": {"compress_gbs": gbs(plain_c), "decompress_gbs": gbs(plain_d),

@@ -269,9 +269,24 @@ mans_status mans_batch_stage_times(mans_batch* b, float ms[6], int calls[2]);
 mans_status mans_batch_get_schedule(const mans_batch* b, int ctas_per_sm[6],
                                     int max_ctas_per_sm[6]);
 mans_status mans_batch_set_schedule(mans_batch* b, const int ctas_per_sm[6]);
-/* Time candidate schedules on this batch (it is compressed several times),
- * keep the fastest whose streams match the default schedule's checksum, and
- * report its time. */
+/* The full schedule, per stage (same order): resident CTAs per SM (the map
+ * stage counts CTAs of 8 warps), warps per CTA (4 or 8 for the map stage, 8
+ * for the others) and the L2 prefetch distance in grids of units ahead (0 to
+ * 2 for the map and encode stages, 0 for the others). Never changes the bytes
+ * produced. limits (may be NULL) receives the largest accepted values. */
+typedef struct mans_batch_schedule {
+  int ctas_per_sm[6];
+  int warps_per_cta[6];
+  int prefetch_grids[6];
+} mans_batch_schedule;
+mans_status mans_batch_get_schedule_ex(const mans_batch* b, mans_batch_schedule* sch,
+                                       mans_batch_schedule* limits);
+mans_status mans_batch_set_schedule_ex(mans_batch* b, const mans_batch_schedule* sch);
+/* Time candidate schedules on this batch (it is compressed several times):
+ * coordinate descent over the map stage's CTAs per SM, warps per CTA and
+ * prefetch distance, then the encode stage's CTAs per SM and prefetch
+ * distance. Keeps the fastest schedule whose streams match the starting
+ * schedule's checksum, and reports its time. */
 mans_status mans_batch_autotune(mans_batch* b, const mans_batch_item* items, uint32_t count,
                                 mans_stream_t stream, float* best_ms);
 

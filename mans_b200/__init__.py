@@ -37,6 +37,14 @@ MANS_U8, MANS_U16, MANS_U32 = 1, 2, 4
 
 # Every symbol include/mans.h declares, with (restype, argtypes).
 _vp, _u64, _u32, _i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int
+class BatchSchedule(C.Structure):
+    """mans_batch_schedule (include/mans.h): per stage (map, plan, encode,
+    decode plan, decode, unmap) resident CTAs per SM, warps per CTA and L2
+    prefetch distance in grids of units ahead."""
+    _fields_ = [("ctas_per_sm", C.c_int * 6), ("warps_per_cta", C.c_int * 6),
+                ("prefetch_grids", C.c_int * 6)]
+
+
 SIGNATURES = {
     "mans_workspace_create": (_i32, [C.POINTER(_vp), _u64, _u64]),
     "mans_workspace_destroy": (_i32, [_vp]),
@@ -72,6 +80,8 @@ SIGNATURES = {
     "mans_batch_stage_times": (_i32, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "mans_batch_get_schedule": (_i32, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "mans_batch_set_schedule": (_i32, [_vp, C.POINTER(C.c_int)]),
+    "mans_batch_get_schedule_ex": (_i32, [_vp, C.POINTER(BatchSchedule), C.POINTER(BatchSchedule)]),
+    "mans_batch_set_schedule_ex": (_i32, [_vp, C.POINTER(BatchSchedule)]),
     "mans_batch_autotune": (_i32, [_vp, _vp, _u32, _vp, C.POINTER(C.c_float)]),
     "mans_clock_ns": (_u64, []),
     "mans_server_create": (_i32, [C.POINTER(_vp), _vp]),

@@ -111,6 +111,25 @@ class Batch:
         arr = (C.c_int * 6)(*ctas_per_sm)
         _check(load().mans_batch_set_schedule(self.h, arr), "mans_batch_set_schedule")
 
+    def schedule_ex(self) -> tuple[dict, dict]:
+        """The full schedule and its limits, each as {"ctas_per_sm": [...],
+        "warps_per_cta": [...], "prefetch_grids": [...]} over the six stages."""
+        from . import BatchSchedule
+        cur, lim = BatchSchedule(), BatchSchedule()
+        _check(load().mans_batch_get_schedule_ex(self.h, C.byref(cur), C.byref(lim)),
+               "mans_batch_get_schedule_ex")
+
+        def as_dict(x):
+            return {f: list(getattr(x, f)) for f, _ in BatchSchedule._fields_}
+        return as_dict(cur), as_dict(lim)
+
+    def set_schedule_ex(self, sch: dict) -> None:
+        from . import BatchSchedule
+        x = BatchSchedule()
+        for f, _ in BatchSchedule._fields_:
+            getattr(x, f)[:] = list(sch[f])
+        _check(load().mans_batch_set_schedule_ex(self.h, C.byref(x)), "mans_batch_set_schedule_ex")
+
     def autotune(self, items, stream=None) -> float:
         ms = C.c_float(0)
         _check(load().mans_batch_autotune(self.h, C.cast(items, C.c_void_p), len(items),

@@ -65,6 +65,9 @@ __global__ void batch_begin_kernel(BatchState* states, uint32_t count, Ctrl* ctr
 struct BatchMapSmem {
   alignas(16) uint8_t stage[kBWarps][kGroupRecMax + 16];
 };
+// dynamic shared memory of the uint32 map for CTAs of `warps` warps (the
+// stages of the warps present)
+inline size_t map32_smem(int warps) { return (size_t)warps * (kGroupRecMax + 16); }
 
 // Histogram merging. Every warp counts into its own shared histogram. When
 // it leaves a buffer, it adds those counts into a CTA-level slot for that
@@ -167,17 +170,19 @@ __global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_m
                                                               BatchState* states, uint32_t count,
                                                               uint64_t total_units, Ctrl* ctrl,
                                                               unsigned long long* flags,
-                                                              uint32_t* hists, uint32_t hist_items) {
+                                                              uint32_t* hists, uint32_t hist_items,
+                                                              uint32_t prefetch_grids) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   __shared__ MapHist mh;
   constexpr int kSlot = 3 + (kDtype == MANS_U8 ? 0 : kDtype == MANS_U16 ? 1 : 2);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  for (int i = t; i < (int)(sizeof(MapHist) / 4); i += kBThreads) reinterpret_cast<uint32_t*>(&mh)[i] = 0;
+  for (int i = t; i < (int)(sizeof(MapHist) / 4); i += blockDim.x) reinterpret_cast<uint32_t*>(&mh)[i] = 0;
   __syncthreads();
   uint32_t* wh = mh.warp[warp];
   int hslot = -1;
   const uint32_t epoch = *((volatile uint32_t*)&ctrl->epoch);
-  const uint64_t ahead = (uint64_t)gridDim.x * kBWarps;
+  // the unit prefetch_grids grids of warps ahead is prefetched into L2
+  const uint64_t ahead = (uint64_t)prefetch_grids * gridDim.x * (blockDim.x >> 5);
   uint32_t it = 0, pit = 0, cur_item = 0xffffffffu;
   auto base = [&](uint32_t i) {
     const BatchItem& x = items[i];
@@ -198,7 +203,7 @@ __global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_m
   while (true) {
     const uint32_t u = warp_claim(&ctrl->tile_counter[kSlot], lane);
     if (u >= total_units) break;
-    if (lane == 0 && (uint64_t)u + ahead < total_units) {
+    if (lane == 0 && ahead && (uint64_t)u + ahead < total_units) {
       pit = owner(pit, (uint64_t)u + ahead);
       const BatchItem& pb = items[pit];
       const uint8_t* pp;
@@ -357,7 +362,8 @@ __global__ __launch_bounds__(kBThreads) void batch_encode_kernel(const BatchItem
                                                                  BatchState* states, uint32_t count,
                                                                  Ctrl* ctrl,
                                                                  unsigned long long* flags,
-                                                                 uint8_t* __restrict__ slots) {
+                                                                 uint8_t* __restrict__ slots,
+                                                                 uint32_t prefetch_grids) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   BatchEncSmem& sm = *reinterpret_cast<BatchEncSmem*>(smem_raw);
   __shared__ int s_last;
@@ -370,11 +376,25 @@ __global__ __launch_bounds__(kBThreads) void batch_encode_kernel(const BatchItem
   const uint64_t total = __ldcg(&ctrl->merged_size);
   uint16_t* sout =
       reinterpret_cast<uint16_t*>(slots + ((uint64_t)blockIdx.x * kBWarps + warp) * kEncSlotBytes);
-  uint32_t it = 0, cur_item = 0xffffffffu;
+  uint32_t it = 0, pit = 0, cur_item = 0xffffffffu;
   auto base = [&](uint32_t i) { return (uint64_t)states[i].unit_base; };
+  // the block prefetch_grids grids of warps ahead is prefetched into L2 (a
+  // second forward cursor finds its buffer)
+  const uint64_t ahead = (uint64_t)prefetch_grids * gridDim.x * kBWarps;
   while (true) {
     const uint32_t u = warp_claim(&ctrl->tile_counter[2], lane);
     if (u >= total) break;
+    if (ahead && (uint64_t)u + ahead < total) {
+      pit = find_item(pit, count, (uint32_t)(u + ahead), base);
+      if (lane == 0) {
+        const BatchItem& pb = items[pit];
+        const BatchState* ps = &states[pit];
+        const uint64_t s0 = (uint64_t)(u + ahead - ps->unit_base) * kAnsBlock;
+        if (s0 < ps->msize)
+          prefetch_l2((pb.dtype == MANS_U8 ? pb.in : pb.m) + s0,
+                      (uint32_t)min_u64(kAnsBlock, ps->msize - s0));
+      }
+    }
     it = find_item(it, count, u, base);
     const BatchItem& b = items[it];
     BatchState* st = &states[it];
@@ -636,7 +656,7 @@ void init_batch_cfg(BatchCfg& c, const LaunchCfg& base) {
   c.sms = base.sms;
   // the map and unmap stages report the occupancy of their heaviest variant
   c.occ[kStageMap] = min(occ((const void*)batch_map_kernel<MANS_U16>, kBThreads, 0),
-                         occ((const void*)batch_map_kernel<MANS_U32>, kBThreads, sizeof(BatchMapSmem)));
+                         occ((const void*)batch_map_kernel<MANS_U32>, kBThreads, map32_smem(kBWarps)));
   c.occ[kStagePlanEnc] = occ((const void*)batch_plan_encode_kernel, 256, 0);
   c.occ[kStageEncode] = occ((const void*)batch_encode_kernel, kBThreads, sizeof(BatchEncSmem));
   c.occ[kStagePlanDec] = occ((const void*)batch_plan_decode_kernel, 32, 0);
@@ -648,10 +668,28 @@ void init_batch_cfg(BatchCfg& c, const LaunchCfg& base) {
   c.occ_u16_map = occ((const void*)batch_map_kernel<MANS_U16>, kBThreads, 0);
   c.occ_u8_map = occ((const void*)batch_map_kernel<MANS_U8>, kBThreads, 0);
   c.occ_u16_unmap = occ((const void*)batch_unmap_kernel<MANS_U16>, kBThreads, 0);
+  c.occ_map4[0] = occ((const void*)batch_map_kernel<MANS_U8>, 128, 0);
+  c.occ_map4[1] = occ((const void*)batch_map_kernel<MANS_U16>, 128, 0);
+  c.occ_map4[2] = occ((const void*)batch_map_kernel<MANS_U32>, 128, map32_smem(4));
 }
 
 uint64_t batch_slot_bytes(const BatchCfg& c) {
   return (uint64_t)c.sms * c.occ[kStageEncode] * kBWarps * kEncSlotBytes;
+}
+
+// Map stage of dtype kind k: grid for the schedule's warps per CTA (the
+// schedule counts CTAs of 8 warps; 4-warp CTAs keep the warps per SM).
+static unsigned map_grid(const BatchCfg& c, int kind, uint64_t units, int extra_occ) {
+  int per_sm = c.ctas_per_sm[kStageMap];
+  if (extra_occ > c.occ[kStageMap]) per_sm = per_sm * extra_occ / c.occ[kStageMap];
+  const int w = c.warps[kStageMap];
+  if (w != kBWarps) {
+    per_sm = per_sm * kBWarps / w;
+    if (per_sm > c.occ_map4[kind]) per_sm = c.occ_map4[kind];
+  }
+  const uint64_t want = div_up_u64(units, (uint64_t)w);
+  const uint64_t cap = (uint64_t)c.sms * (uint64_t)(per_sm > 0 ? per_sm : 1);
+  return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
 }
 
 static unsigned grid_of(const BatchCfg& c, int stage, uint64_t want, int extra_occ = 0) {
@@ -667,26 +705,25 @@ cudaError_t launch_batch_compress(const BatchDev& d, uint32_t count, const uint6
                                   cudaEvent_t* marks) {
   if (marks) cudaEventRecord(marks[0], s);
   batch_begin_kernel<<<(count + 255) / 256 + 1, 256, 0, s>>>(d.states, count, d.ctrl);
+  const int mw = c.warps[kStageMap];
+  const uint32_t mpf = (uint32_t)c.prefetch[kStageMap];
   if (groups[1])
-    batch_map_kernel<MANS_U16><<<grid_of(c, kStageMap, div_up_u64(groups[1], kBWarps), c.occ_u16_map),
-                                 kBThreads, 0, s>>>(d.items, d.states, count, groups[1], d.ctrl,
-                                                    d.group_flags, d.hists, d.hist_items);
+    batch_map_kernel<MANS_U16><<<map_grid(c, 1, groups[1], c.occ_u16_map), 32 * mw, 0, s>>>(
+        d.items, d.states, count, groups[1], d.ctrl, d.group_flags, d.hists, d.hist_items, mpf);
   if (groups[2])
-    batch_map_kernel<MANS_U32><<<grid_of(c, kStageMap, div_up_u64(groups[2], kBWarps)), kBThreads,
-                                 sizeof(BatchMapSmem), s>>>(d.items, d.states, count, groups[2],
-                                                            d.ctrl, d.group_flags, d.hists,
-                                                            d.hist_items);
+    batch_map_kernel<MANS_U32><<<map_grid(c, 2, groups[2], 0), 32 * mw, map32_smem(mw), s>>>(
+        d.items, d.states, count, groups[2], d.ctrl, d.group_flags, d.hists, d.hist_items, mpf);
   if (groups[0])
-    batch_map_kernel<MANS_U8><<<grid_of(c, kStageMap, div_up_u64(groups[0], kBWarps), c.occ_u8_map),
-                                kBThreads, 0, s>>>(d.items, d.states, count, groups[0], d.ctrl,
-                                                   d.group_flags, d.hists, d.hist_items);
+    batch_map_kernel<MANS_U8><<<map_grid(c, 0, groups[0], c.occ_u8_map), 32 * mw, 0, s>>>(
+        d.items, d.states, count, groups[0], d.ctrl, d.group_flags, d.hists, d.hist_items, mpf);
   if (marks) cudaEventRecord(marks[1], s);
   batch_plan_encode_kernel<<<grid_of(c, kStagePlanEnc, count), 256, 0, s>>>(
       d.items, d.states, count, d.ctrl, d.item_flags, d.hists, d.hist_items);
   if (marks) cudaEventRecord(marks[2], s);
   batch_encode_kernel<<<grid_of(c, kStageEncode, div_up_u64(max_blocks, kBWarps)), kBThreads,
                         sizeof(BatchEncSmem), s>>>(d.items, d.states, count, d.ctrl,
-                                                   d.block_flags, d.slots);
+                                                   d.block_flags, d.slots,
+                                                   (uint32_t)c.prefetch[kStageEncode]);
   if (marks) cudaEventRecord(marks[3], s);
   return cudaGetLastError();
 }

@@ -381,6 +381,42 @@ mans_status mans_batch_set_schedule(mans_batch* b, const int ctas_per_sm[6]) {
   return MANS_OK;
 }
 
+mans_status mans_batch_get_schedule_ex(const mans_batch* b, mans_batch_schedule* sch,
+                                       mans_batch_schedule* limits) {
+  if (!b) return MANS_ERR_INVALID_ARG;
+  for (int s = 0; s < kStages; ++s) {
+    if (sch) {
+      sch->ctas_per_sm[s] = b->cfg.ctas_per_sm[s];
+      sch->warps_per_cta[s] = b->cfg.warps[s];
+      sch->prefetch_grids[s] = b->cfg.prefetch[s];
+    }
+    if (limits) {
+      limits->ctas_per_sm[s] = b->cfg.occ[s];
+      limits->warps_per_cta[s] = 8;
+      limits->prefetch_grids[s] = (s == kStageMap || s == kStageEncode) ? kMaxPrefetch : 0;
+    }
+  }
+  return MANS_OK;
+}
+
+mans_status mans_batch_set_schedule_ex(mans_batch* b, const mans_batch_schedule* sch) {
+  if (!b || !sch) return MANS_ERR_INVALID_ARG;
+  for (int s = 0; s < kStages; ++s) {
+    const bool tunable_pf = s == kStageMap || s == kStageEncode;
+    if (sch->ctas_per_sm[s] < 1 || sch->ctas_per_sm[s] > b->cfg.occ[s]) return MANS_ERR_INVALID_ARG;
+    if (sch->warps_per_cta[s] != 8 && !(s == kStageMap && sch->warps_per_cta[s] == 4))
+      return MANS_ERR_INVALID_ARG;
+    if (sch->prefetch_grids[s] < 0 || sch->prefetch_grids[s] > (tunable_pf ? kMaxPrefetch : 0))
+      return MANS_ERR_INVALID_ARG;
+  }
+  for (int s = 0; s < kStages; ++s) {
+    b->cfg.ctas_per_sm[s] = sch->ctas_per_sm[s];
+    b->cfg.warps[s] = sch->warps_per_cta[s];
+    b->cfg.prefetch[s] = sch->prefetch_grids[s];
+  }
+  return MANS_OK;
+}
+
 mans_status mans_batch_autotune(mans_batch* b, const mans_batch_item* items, uint32_t count,
                                 mans_stream_t stream, float* best_ms) {
   if (!b) return MANS_ERR_INVALID_ARG;
@@ -396,41 +432,69 @@ mans_status mans_batch_autotune(mans_batch* b, const mans_batch_item* items, uin
   unsigned long long ref_sum = 0;
   bool have_ref = false;
   mans_status st = MANS_OK;
-  // candidate resident CTAs per SM for the two heavy compress stages
-  std::vector<int> cm, ce;
-  for (int v = start.occ[kStageMap]; v >= 1; v = v > 2 ? v / 2 : v - 1) cm.push_back(v);
-  for (int v = start.occ[kStageEncode]; v >= 1; v = v > 2 ? v / 2 : v - 1) ce.push_back(v);
-  for (int m : cm) {
-    for (int en : ce) {
-      b->cfg = start;
-      b->cfg.ctas_per_sm[kStageMap] = m;
-      b->cfg.ctas_per_sm[kStageEncode] = en;
-      float tm = 0;
-      for (int rep = 0; rep < 2 && st == MANS_OK; ++rep) {  // first run warms up
-        cudaEventRecord(e0, s);
-        st = mans_batch_compress(b, items, count, stream);
-        cudaEventRecord(e1, s);
-        if (cudaEventSynchronize(e1) != cudaSuccess) st = MANS_ERR_CUDA;
-        cudaEventElapsedTime(&tm, e0, e1);
-      }
-      if (st != MANS_OK) break;
-      cudaMemsetAsync(d_sum, 0, sizeof(unsigned long long), s);
-      batch_checksum_kernel<<<b->cfg.sms, 256, 0, s>>>(b->dev.items, b->dev.states, count, d_sum);
-      unsigned long long sum = 0;
-      cudaMemcpyAsync(&sum, d_sum, sizeof(sum), cudaMemcpyDeviceToHost, s);
-      cudaStreamSynchronize(s);
-      if (!have_ref) {
-        ref_sum = sum;
-        have_ref = true;
-      } else if (sum != ref_sum) {
-        continue;  // a schedule that changed the bytes is never chosen
-      }
-      if (tm < best_t) {
-        best_t = tm;
-        best = b->cfg;
-      }
+  // Time one schedule (the first of two runs warms up) and keep it when it
+  // is faster and its streams' checksum equals the starting schedule's.
+  auto trial = [&](const BatchCfg& cand) {
+    if (st != MANS_OK) return;
+    b->cfg = cand;
+    float tm = 0;
+    for (int rep = 0; rep < 2 && st == MANS_OK; ++rep) {
+      cudaEventRecord(e0, s);
+      st = mans_batch_compress(b, items, count, stream);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) st = MANS_ERR_CUDA;
+      cudaEventElapsedTime(&tm, e0, e1);
     }
-    if (st != MANS_OK) break;
+    if (st != MANS_OK) return;
+    cudaMemsetAsync(d_sum, 0, sizeof(unsigned long long), s);
+    batch_checksum_kernel<<<b->cfg.sms, 256, 0, s>>>(b->dev.items, b->dev.states, count, d_sum);
+    unsigned long long sum = 0;
+    cudaMemcpyAsync(&sum, d_sum, sizeof(sum), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      st = MANS_ERR_CUDA;
+      return;
+    }
+    if (!have_ref) {
+      ref_sum = sum;
+      have_ref = true;
+    } else if (sum != ref_sum) {
+      return;  // a schedule that changed the bytes is never chosen
+    }
+    if (tm < best_t) {
+      best_t = tm;
+      best = cand;
+    }
+  };
+  auto halvings = [](int top) {
+    std::vector<int> v;
+    for (int x = top; x >= 1; x = x > 2 ? x / 2 : x - 1) v.push_back(x);
+    return v;
+  };
+  trial(start);
+  for (int m : halvings(start.occ[kStageMap])) {  // map: resident CTAs per SM
+    BatchCfg c = best;
+    c.ctas_per_sm[kStageMap] = m;
+    if (m != best.ctas_per_sm[kStageMap]) trial(c);
+  }
+  {  // map: warps per CTA
+    BatchCfg c = best;
+    c.warps[kStageMap] = best.warps[kStageMap] == 8 ? 4 : 8;
+    trial(c);
+  }
+  for (int pf = 0; pf <= kMaxPrefetch; ++pf) {  // map: prefetch distance
+    BatchCfg c = best;
+    c.prefetch[kStageMap] = pf;
+    if (pf != best.prefetch[kStageMap]) trial(c);
+  }
+  for (int en : halvings(start.occ[kStageEncode])) {  // encode: resident CTAs per SM
+    BatchCfg c = best;
+    c.ctas_per_sm[kStageEncode] = en;
+    if (en != best.ctas_per_sm[kStageEncode]) trial(c);
+  }
+  for (int pf = 0; pf <= kMaxPrefetch; ++pf) {  // encode: prefetch distance
+    BatchCfg c = best;
+    c.prefetch[kStageEncode] = pf;
+    if (pf != best.prefetch[kStageEncode]) trial(c);
   }
   b->cfg = st == MANS_OK ? best : start;
   // leave the outputs of the chosen schedule in place

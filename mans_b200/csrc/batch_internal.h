@@ -67,15 +67,24 @@ enum BatchStage {
   kStages
 };
 
-// Schedule of the batched kernels: resident CTAs per SM of each stage
-// (ctas_per_sm <= occ). The bytes produced do not depend on it.
+// Schedule of the batched kernels. The bytes produced do not depend on it.
+//   ctas_per_sm: resident CTAs per SM of each stage (<= occ); for the map
+//     stage counted in CTAs of 8 warps, whatever its warps per CTA.
+//   warps: warps per CTA (the map stage takes 4 or 8; the others 8).
+//   prefetch: L2 prefetch distance of the map and encode stages, in grids of
+//     units ahead (0: none; at most kMaxPrefetch).
 struct BatchCfg {
   int sms = 148;
   int occ[kStages] = {1, 1, 1, 1, 1, 1};
   int ctas_per_sm[kStages] = {1, 1, 1, 1, 1, 1};
+  int warps[kStages] = {8, 8, 8, 8, 8, 8};
+  int prefetch[kStages] = {1, 0, 0, 0, 0, 0};
   // occupancy of the lighter map / unmap variants (grids scale with it)
   int occ_u16_map = 1, occ_u8_map = 1, occ_u16_unmap = 1;
+  // occupancy of the 4-warp map variants, by dtype kind (u8, u16, u32)
+  int occ_map4[3] = {1, 1, 1};
 };
+constexpr int kMaxPrefetch = 2;
 
 void init_batch_cfg(BatchCfg& c, const LaunchCfg& base);
 uint64_t batch_slot_bytes(const BatchCfg& c);

@@ -259,3 +259,40 @@ def test_batch_schedule_and_autotune_keep_bytes(ws, torch_cuda):
             np.testing.assert_array_equal(s, r)
     finally:
         b.close()
+
+
+def test_batch_full_schedule_keeps_bytes(ws, torch_cuda):
+    """Warps per CTA of the map stage (4 or 8) and the L2 prefetch distance of
+    the map and encode stages change the schedule only: every stream equals
+    the single-buffer path's and decodes back."""
+    b = Batch(64, 64 << 20)
+    try:
+        xs = mixed(11, list(W.mixed_sizes(30, seed=11, lo=4 << 10, hi=2 << 20) // 4) + EDGE)
+        ref = [single_stream(ws, x, 10) for x in xs]
+        cur, lim = b.schedule_ex()
+        assert cur["warps_per_cta"] == [8] * 6
+        assert lim["prefetch_grids"][0] == 2 and lim["prefetch_grids"][2] == 2
+        for warps, pf_map, pf_enc, frac in ((4, 0, 0, 1), (4, 2, 1, 2), (8, 0, 2, 1), (4, 1, 2, 4)):
+            sch = {k: list(v) for k, v in cur.items()}
+            sch["warps_per_cta"][0] = warps
+            sch["prefetch_grids"][0] = pf_map
+            sch["prefetch_grids"][2] = pf_enc
+            sch["ctas_per_sm"] = [max(1, m // frac) for m in lim["ctas_per_sm"]]
+            b.set_schedule_ex(sch)
+            assert b.schedule_ex()[0] == sch
+            first, st, streams = run_compress(b, xs, [10] * len(xs))
+            assert first == 0, (sch, st)
+            for i, (r, s) in enumerate(zip(ref, streams)):
+                np.testing.assert_array_equal(s, r, err_msg=f"{sch} item {i}")
+            first, st, back = run_decompress(b, streams, xs)
+            assert first == 0
+            for x, y in zip(xs, back):
+                np.testing.assert_array_equal(y, x)
+        for bad in ({"warps_per_cta": [6, 8, 8, 8, 8, 8]}, {"warps_per_cta": [8, 4, 8, 8, 8, 8]},
+                    {"prefetch_grids": [3, 0, 0, 0, 0, 0]}, {"prefetch_grids": [0, 1, 0, 0, 0, 0]}):
+            sch = {k: list(v) for k, v in cur.items()}
+            sch.update(bad)
+            with pytest.raises(mb.MansError):
+                b.set_schedule_ex(sch)
+    finally:
+        b.close()
