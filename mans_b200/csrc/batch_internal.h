@@ -78,7 +78,7 @@ struct BatchCfg {
   int occ[kStages] = {1, 1, 1, 1, 1, 1};
   int ctas_per_sm[kStages] = {1, 1, 1, 1, 1, 1};
   int warps[kStages] = {8, 8, 8, 8, 8, 8};
-  int prefetch[kStages] = {1, 0, 0, 0, 0, 0};
+  int prefetch[kStages] = {0, 0, 0, 0, 0, 0};
   // occupancy of the lighter map / unmap variants (grids scale with it)
   int occ_u16_map = 1, occ_u8_map = 1, occ_u16_unmap = 1;
   // occupancy of the 4-warp map variants, by dtype kind (u8, u16, u32)
