@@ -24,8 +24,10 @@ def ws():
     w.close()
 
 
-def _u16(rng, n: int) -> np.ndarray:
+def _u16(rng, n: int, full_range: bool = True) -> np.ndarray:
     fam = int(rng.integers(0, 6))
+    if fam == 3 and not full_range:
+        fam = 0
     seed = int(rng.integers(1 << 30))
     if fam == 0:
         b = float(rng.choice([2.0, 40.0, 400.0, 4000.0]))
@@ -89,3 +91,50 @@ def test_random_case_matches_oracle(ws, oracle, case):
     tdt = {np.uint8: torch.uint8, np.uint16: torch.uint16, np.uint32: torch.uint32}[x.dtype.type]
     y = mb.decompress(to_dev(s), x.size, tdt, ws=ws, layout=layout)
     np.testing.assert_array_equal(to_host(y, x.dtype), x, err_msg=what)
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_random_batch_matches_oracle(ws, oracle, seed):
+    """40 random buffers of mixed type in one batched call per direction."""
+    import torch
+
+    from mans_b200.batch import Batch
+    rng = np.random.default_rng(9100 + seed)
+    xs, ps = [], []
+    for i in range(40):
+        kind = ("u8", "u16", "u32")[int(rng.integers(0, 3))]
+        n = int(np.exp(rng.uniform(0.0, np.log(600_000))))
+        if kind == "u8":
+            xs.append(W.random_bytes(n, int(rng.integers(1 << 30)),
+                                     str(rng.choice(["skewed", "uniform", "two", "sparse"]))))
+        elif kind == "u16":
+            # no full-range uint16: a small one maps to up to ~33x its bytes, past
+            # the per-buffer room of any fixed ratio (it then fails alone)
+            xs.append(_u16(rng, n, full_range=False))
+        else:
+            xs.append(_u32(rng, n))
+        ps.append(int(rng.integers(9, 12)))
+    refs = [oracle.ans_encode(x, p) if x.dtype == np.uint8 else oracle.compress(x, p)
+            for x, p in zip(xs, ps)]
+    tdt = {np.uint8: torch.uint8, np.uint16: torch.uint16, np.uint32: torch.uint32}
+    # wide uint16 spreads map to up to ~8x their bytes here; the default room
+    # (210%) would fail those buffers alone with MANS_ERR_WORKSPACE_OVERFLOW
+    b = Batch(64, 64 << 20, 1000)
+    try:
+        dx = [to_dev(x) for x in xs]
+        outs = [torch.empty(mb.max_compressed_size(mb.dtype_code(d), d.numel()),
+                            dtype=torch.uint8, device="cuda") for d in dx]
+        sizes = torch.zeros(len(xs), dtype=torch.int64, device="cuda")
+        b.compress_async(Batch.compress_items(dx, outs, sizes, ps))
+        b.check(len(xs), what="random batch compress")
+        streams = [to_host(o[: int(n)]) for o, n in zip(outs, sizes.tolist())]
+        for i, (s, r) in enumerate(zip(streams, refs)):
+            np.testing.assert_array_equal(s, r, err_msg=f"seed {seed} item {i} {xs[i].dtype} n={xs[i].size}")
+        ds = [to_dev(s) for s in streams]
+        backs = [torch.empty(x.size, dtype=tdt[x.dtype.type], device="cuda") for x in xs]
+        b.decompress_async(Batch.decompress_items(ds, [s.size for s in streams], backs))
+        b.check(len(xs), what="random batch decompress")
+        for i, (x, y) in enumerate(zip(xs, backs)):
+            np.testing.assert_array_equal(to_host(y, x.dtype), x, err_msg=f"seed {seed} item {i}")
+    finally:
+        b.close()
