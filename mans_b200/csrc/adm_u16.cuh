@@ -90,29 +90,31 @@ __device__ __forceinline__ void load_lane_u16(const uint16_t* __restrict__ in, u
   }
 }
 
-// Map group `grp` of one buffer (one warp). flags: the buffer's per-group
-// look-back flags; msize_out: written by the buffer's last group; hist: the
-// warp's shared histogram.
+// One lane's share of a mapped group between the two halves of the map.
+struct Map16Lane {
+  uint64_t acc;   // the lane's first 64 stream bits (tail-filled when shorter)
+  uint32_t pos;   // the lane's stream bits
+  uint32_t L;     // the group's lane length in bytes (the longest lane)
+  uint32_t c;     // the group's center
+  int cnt;        // valid elements of the lane
+};
+
+// First half of mapping group `grp` (one warp): everything that does not
+// depend on the group's offset -- center, codes (stored), the lane bit
+// streams' first 64 bits, the group length and the histogram of the codes
+// and of a short lane's bit bytes. hist: the warp's shared histogram.
 template <int kLayout = kLayoutV15>
-__device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uint64_t n,
-                                            uint8_t* __restrict__ M, uint64_t m_cap,
-                                            unsigned long long* flags,
-                                            unsigned long long* msize_out, uint32_t grp,
-                                            uint32_t epoch, const Sink& sink, uint32_t* hist,
-                                            int lane) {
+__device__ __forceinline__ void map16_front(const uint16_t* __restrict__ in, uint64_t n,
+                                            uint8_t* __restrict__ M, uint32_t grp,
+                                            uint32_t* hist, int lane, Map16Lane& a) {
   const uint64_t g = div_up_u64(n, kAdmGroup);
-  const uint64_t hdr = u16_header_bytes(kLayout, g);
-  uint8_t* p_len = M;
-  uint8_t* p_ctr = M + u16_len_bytes(kLayout, g);
-  uint8_t* p_code = M + hdr;
-  uint8_t* p_bits = M + hdr + n;
-  const uint64_t bits_base = hdr + n;  // offset of the bits section in M
+  uint8_t* p_code = M + u16_header_bytes(kLayout, g);
   uint32_t w[8];
   load_lane_u16(in, n, grp, lane, w);
 
   const uint64_t gs = (uint64_t)grp * kAdmGroup;
   const uint64_t ls = gs + (uint64_t)lane * kAdmChunk;
-  const int cnt = ls >= n ? 0 : (int)min_u64(16, n - ls);
+  a.cnt = ls >= n ? 0 : (int)min_u64(16, n - ls);
 
   // ---- center: truncated mean (u32 sum of at most 512 uint16 values)
   uint32_t lsum = 0;
@@ -120,7 +122,7 @@ __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uin
   for (int i = 0; i < 8; ++i) lsum += (w[i] & 0xffffu) + (w[i] >> 16);
   const uint32_t gsum = __reduce_add_sync(0xffffffffu, lsum);
   const uint32_t gcnt = (uint32_t)min_u64(kAdmGroup, n - gs);
-  const uint32_t c = gcnt == kAdmGroup ? (gsum >> 9) : gsum / gcnt;
+  a.c = gcnt == kAdmGroup ? (gsum >> 9) : gsum / gcnt;
 
   // ---- map: codes, unary bits (first 64 bits in a register), lane length
   uint32_t codes[4] = {0, 0, 0, 0};
@@ -128,48 +130,57 @@ __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uin
   uint32_t pos = 0;
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
-    if (i < cnt) {
+    if (i < a.cnt) {
       uint32_t k, code;
-      adm_elem_u16(elem16(w, i), c, k, code);
+      adm_elem_u16(elem16(w, i), a.c, k, code);
       codes[i >> 2] |= code << ((i & 3) * 8);
       atomicAdd(&hist[code], 1u);
       if (pos < 64) acc |= 0x8000000000000000ull >> pos;
       pos += k;
     }
   }
-  const uint32_t L = __reduce_max_sync(0xffffffffu, (pos + 7) >> 3);
-
-  // ---- publish the group length now; the prefix is read after the work
-  //      that does not depend on it
-  if (lane == 0) st_flag(&flags[grp], make_flag(grp == 0 ? kFlagIncl : kFlagAgg, epoch, L));
+  a.L = __reduce_max_sync(0xffffffffu, (pos + 7) >> 3);
+  a.pos = pos;
 
   // codes: 16-byte aligned (the codes section is aligned by the caller)
-  if (cnt == 16) {
+  if (a.cnt == 16) {
     *reinterpret_cast<uint4*>(p_code + ls) = make_uint4(codes[0], codes[1], codes[2], codes[3]);
   } else {
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-      if (i < cnt) p_code[ls + i] = (uint8_t)(codes[i >> 2] >> ((i & 3) * 8));
+      if (i < a.cnt) p_code[ls + i] = (uint8_t)(codes[i >> 2] >> ((i & 3) * 8));
   }
   // bit bytes of a short lane (< 64 bits): tail fill and histogram now. In
   // the V12 layout a lane without elements is all 0xFF.
-  const bool fast = pos < 64;
-  const bool v12_empty = kLayout == kLayoutV12 && cnt == 0;
-  const uint32_t rest = v12_empty ? 0xffu : 0u;  // bytes past the first 8
-  if (fast) {
+  const bool v12_empty = kLayout == kLayoutV12 && a.cnt == 0;
+  if (pos < 64) {
     if (v12_empty) acc = ~0ull;
-    else if (pos < 8 * L) acc |= tail_fill_mask(pos);
-    const uint32_t nb8 = L < 8 ? L : 8u;
+    else if (pos < 8 * a.L) acc |= tail_fill_mask(pos);
+    const uint32_t nb8 = a.L < 8 ? a.L : 8u;
     for (uint32_t b = 0; b < nb8; ++b) atomicAdd(&hist[(uint32_t)(acc >> (56 - 8 * b)) & 0xffu], 1u);
-    if (L > 8) atomicAdd(&hist[rest], L - 8);
+    if (a.L > 8) atomicAdd(&hist[v12_empty ? 0xffu : 0u], a.L - 8);
   }
+  a.acc = acc;
+}
 
-  // ---- group bit offset (in units of 32 bytes)
-  uint32_t gexcl = 0;
-  if (grp > 0) {
-    gexcl = lookback_exclusive(flags, grp, epoch, sink);
-    if (lane == 0) st_flag(&flags[grp], make_flag(kFlagIncl, epoch, gexcl + L));
-  }
+// Second half, once the group's bit offset gexcl (in units of 32 bytes) is
+// known: the merged size (last group), the group's length (or prefix) and
+// center fields with their histogram counts, and the lanes' bit bytes. A
+// long lane (64 bits or more) reloads its elements and regenerates its
+// stream byte by byte.
+template <int kLayout = kLayoutV15>
+__device__ __forceinline__ void map16_back(const uint16_t* __restrict__ in, uint64_t n,
+                                           uint8_t* __restrict__ M, uint64_t m_cap,
+                                           unsigned long long* msize_out, uint32_t grp,
+                                           uint32_t gexcl, const Map16Lane& a, const Sink& sink,
+                                           uint32_t* hist, int lane) {
+  const uint64_t g = div_up_u64(n, kAdmGroup);
+  const uint64_t hdr = u16_header_bytes(kLayout, g);
+  uint8_t* p_len = M;
+  uint8_t* p_ctr = M + u16_len_bytes(kLayout, g);
+  uint8_t* p_bits = M + hdr + n;
+  const uint64_t bits_base = hdr + n;  // offset of the bits section in M
+  const uint32_t L = a.L, c = a.c, pos = a.pos;
   if (lane == 0 && (uint64_t)grp + 1 == g) {
     const unsigned long long msize = bits_base + 32ull * (gexcl + L);
     *msize_out = msize;
@@ -208,15 +219,18 @@ __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uin
   const uint64_t gend = bits_base + 32ull * ((uint64_t)gexcl + L);
   if (gend <= m_cap) {
     uint8_t* dst = p_bits + 32ull * gexcl + (uint64_t)lane * L;
-    if (fast) {
+    if (pos < 64) {
+      const uint32_t rest = (kLayout == kLayoutV12 && a.cnt == 0) ? 0xffu : 0u;
       for (uint32_t b = 0; b < L; ++b)
-        dst[b] = (uint8_t)(b < 8 ? (uint32_t)(acc >> (56 - 8 * b)) & 0xffu : rest);
+        dst[b] = (uint8_t)(b < 8 ? (uint32_t)(a.acc >> (56 - 8 * b)) & 0xffu : rest);
     } else {
       // Long lane: regenerate the stream byte by byte.
+      uint32_t w[8];
+      load_lane_u16(in, n, grp, lane, w);
       uint32_t cur = 0, bi = 0, bp = 0;
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        if (i < cnt) {
+        if (i < a.cnt) {
           uint32_t k, code;
           adm_elem_u16(elem16(w, i), c, k, code);
           while ((bp >> 3) > bi) {
@@ -244,6 +258,29 @@ __device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uin
       }
     }
   }
+}
+
+// Map group `grp` of one buffer (one warp) with a per-group look-back.
+// flags: the buffer's per-group look-back flags; msize_out: written by the
+// buffer's last group; hist: the warp's shared histogram. The group length is
+// published as soon as it is known; the prefix is read after the work that
+// does not depend on it.
+template <int kLayout = kLayoutV15>
+__device__ __forceinline__ void map16_group(const uint16_t* __restrict__ in, uint64_t n,
+                                            uint8_t* __restrict__ M, uint64_t m_cap,
+                                            unsigned long long* flags,
+                                            unsigned long long* msize_out, uint32_t grp,
+                                            uint32_t epoch, const Sink& sink, uint32_t* hist,
+                                            int lane) {
+  Map16Lane a;
+  map16_front<kLayout>(in, n, M, grp, hist, lane, a);
+  if (lane == 0) st_flag(&flags[grp], make_flag(grp == 0 ? kFlagIncl : kFlagAgg, epoch, a.L));
+  uint32_t gexcl = 0;
+  if (grp > 0) {
+    gexcl = lookback_exclusive(flags, grp, epoch, sink);
+    if (lane == 0) st_flag(&flags[grp], make_flag(kFlagIncl, epoch, gexcl + a.L));
+  }
+  map16_back<kLayout>(in, n, M, m_cap, msize_out, grp, gexcl, a, sink, hist, lane);
 }
 
 // ------------------------------------------------------------------------
