@@ -15,7 +15,7 @@ namespace mans {
 // are claimed in order, one at a time (a claim held while another unit is
 // mapped would stall every later unit's look-back), and the unit one grid of
 // warps ahead is prefetched into L2 for whichever warp claims it.
-constexpr uint32_t kMapUnit = 2;
+constexpr uint32_t kMapUnit = kU16MapUnit;
 
 template <int kLayout>
 __global__ __launch_bounds__(kMapThreads, 5) void adm_u16_map_kernel(

@@ -159,7 +159,9 @@ template <uint32_t kDtype>
 __device__ __forceinline__ void unit_span(const BatchItem& b, uint64_t u, const uint8_t*& p,
                                           uint32_t& bytes) {
   constexpr uint32_t eb = kDtype == MANS_U8 ? 1 : kDtype == MANS_U16 ? 2 : 4;
-  constexpr uint32_t per = kDtype == MANS_U8 ? kRawChunk : kAdmGroup;
+  constexpr uint32_t per = kDtype == MANS_U8    ? kRawChunk
+                           : kDtype == MANS_U16 ? kU16MapUnit * kAdmGroup
+                                                : kAdmGroup;
   const uint64_t s0 = u * per;
   p = b.in + s0 * eb;
   bytes = (uint32_t)(min_u64(per, b.n - s0) * eb);
@@ -223,8 +225,33 @@ __global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_m
     const Sink sink = item_sink(ctrl, st);
     const uint32_t grp = (uint32_t)(u - b.group_base);
     if constexpr (kDtype == MANS_U16) {
-      map16_group(reinterpret_cast<const uint16_t*>(b.in), b.n, b.m, b.m_cap, flags + b.flag_base,
-                  &st->msize, grp, epoch, sink, wh, lane);
+      // unit grp: groups kU16MapUnit * grp + q of the buffer, one look-back
+      const uint16_t* in16 = reinterpret_cast<const uint16_t*>(b.in);
+      const uint64_t g = div_up_u64(b.n, kAdmGroup);
+      unsigned long long* fl = flags + b.flag_base;
+      Map16Lane S[kU16MapUnit];
+      uint32_t len = 0;
+#pragma unroll
+      for (uint32_t q = 0; q < kU16MapUnit; ++q) {
+        S[q].L = 0;
+        if ((uint64_t)grp * kU16MapUnit + q < g) {
+          map16_front(in16, b.n, b.m, grp * kU16MapUnit + q, wh, lane, S[q]);
+          len += S[q].L;
+        }
+      }
+      if (lane == 0) st_flag(&fl[grp], make_flag(grp == 0 ? kFlagIncl : kFlagAgg, epoch, len));
+      uint32_t off = 0;
+      if (grp > 0) {
+        off = lookback_exclusive(fl, grp, epoch, sink);
+        if (lane == 0) st_flag(&fl[grp], make_flag(kFlagIncl, epoch, off + len));
+      }
+#pragma unroll
+      for (uint32_t q = 0; q < kU16MapUnit; ++q) {
+        if ((uint64_t)grp * kU16MapUnit + q < g)
+          map16_back(in16, b.n, b.m, b.m_cap, &st->msize, grp * kU16MapUnit + q, off, S[q], sink,
+                     wh, lane);
+        off += S[q].L;
+      }
     } else if constexpr (kDtype == MANS_U32) {
       BatchMapSmem& sm = *reinterpret_cast<BatchMapSmem*>(smem_raw);
       map32_group(reinterpret_cast<const uint32_t*>(b.in), b.n, b.m, b.m_cap, flags + b.flag_base,

@@ -103,8 +103,11 @@ mans_status layout(mans_batch* b, const mans_batch_item* items, uint32_t count, 
       off += align_up(cap + kItemSlack, 256);
       blocks = div_up_u64(cap, kAnsBlock);
     }
-    groups[kind] += g;
-    flags += g;
+    // compress: the uint16 map claims (and looks back over) units of
+    // kU16MapUnit groups; decompress: the unmap takes single groups
+    const uint64_t claims = (compress && it.dtype == MANS_U16) ? div_up_u64(g, kU16MapUnit) : g;
+    groups[kind] += claims;
+    flags += claims;
     units += blocks;
     chunks += div_up_u64(blocks, 8);
   }

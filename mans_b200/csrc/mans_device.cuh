@@ -34,6 +34,9 @@ constexpr int kAdmChunk = 16;     // elements per lane
 constexpr int kAdmGroup = 512;    // elements per group (one warp)
 constexpr uint32_t kAdmStep = 126;
 constexpr int kAdmGroupsPerTile = 8;  // warps (groups in flight) per CTA of the mappers
+// uint16 groups per unit of the map's claims and look-back (a uint16 group is
+// 1 KiB of input; two halve the per-byte cost of claims and look-backs).
+constexpr uint32_t kU16MapUnit = 2;
 
 // ---- device status (first error wins) ----
 struct Ctrl {
