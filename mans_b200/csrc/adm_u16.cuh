@@ -346,19 +346,22 @@ __device__ __forceinline__ void unmap16_group(const uint8_t* __restrict__ M, uin
   if (L <= 8) {
     uint64_t acc = 0;
     for (uint32_t b = 0; b < L; ++b) acc |= (uint64_t)src[b] << (56 - 8 * b);
-    const int nbits = 8 * (int)L;
-    int pos = 0;  // stream position of the current element's leading 1
+    // win: the stream from the current element's leading 1, left-aligned;
+    // left: its bits that are still in the lane's record
+    uint64_t win = acc;
+    int left = 8 * (int)L;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       sig[i] = 0;
       if (i < cnt) {
-        if (pos >= nbits || !((acc << pos) >> 63)) bad = true;
-        const uint64_t rest = pos + 1 < 64 ? (acc << (pos + 1)) : 0ull;
+        if (left <= 0 || !(win >> 63)) bad = true;
+        const uint64_t rest = win << 1;
         int z = rest ? __clzll(rest) : 64;
-        const int left = nbits - pos - 1;
-        z = z < left ? z : (left > 0 ? left : 0);
+        const int lim = left > 1 ? left - 1 : 0;
+        z = z < lim ? z : lim;
         sig[i] = (uint32_t)z;
-        pos += z + 1;
+        win = z < 63 ? rest << z : 0ull;  // advance by z + 1 bits
+        left -= z + 1;
       }
     }
   } else {
