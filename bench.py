@@ -474,21 +474,46 @@ def run_mans(args):
             "h_out": torch.zeros(U, dtype=torch.uint8, pin_memory=True),
             "ev": torch.cuda.Event()})
 
+    # Each buffer set has an upload, a download and a kernel stream, so that
+    # a set's next upload overlaps its previous download and no copy waits
+    # behind another set's copies. Events order every use of a set's buffers
+    # after the previous use is finished.
+    for S in sets:
+        S["up"], S["down"] = torch.cuda.Stream(), torch.cuda.Stream()
+        for e in ("e_in", "e_c", "e_size", "e_sd", "e_su", "e_dc", "e_free"):
+            S[e] = torch.cuda.Event()
+
     def first_half(S):
-        with torch.cuda.stream(S["s"]):
+        S["up"].wait_event(S["e_c"])  # the set's previous compress has read d_in
+        with torch.cuda.stream(S["up"]):
             S["d_in"].view(torch.uint8).copy_(h_in, non_blocking=True)
-            mb.compress_into(S["ws"], S["d_in"], S["out"], S["size"], args.precision, S["s"])
+            S["e_in"].record(S["up"])
+        S["s"].wait_event(S["e_in"])
+        S["s"].wait_event(S["e_free"])  # the previous step's out / d_back are read
+        mb.compress_into(S["ws"], S["d_in"], S["out"], S["size"], args.precision, S["s"])
+        S["e_c"].record(S["s"])
+        S["down"].wait_event(S["e_c"])
+        with torch.cuda.stream(S["down"]):
             S["h_size"].copy_(S["size"], non_blocking=True)
-            S["ev"].record(S["s"])
+            S["e_size"].record(S["down"])
 
     def second_half(S):
-        S["ev"].synchronize()  # the compressed size, read on the host
+        S["e_size"].synchronize()  # the compressed size, read on the host
         c = int(S["h_size"].item())
-        with torch.cuda.stream(S["s"]):
+        with torch.cuda.stream(S["down"]):
             S["h_s"][:c].copy_(S["out"][:c], non_blocking=True)
+            S["e_sd"].record(S["down"])
+        S["up"].wait_event(S["e_sd"])
+        with torch.cuda.stream(S["up"]):
             S["d_s"][:c].copy_(S["h_s"][:c], non_blocking=True)
-            mb.decompress_into(S["ws"], S["d_s"], c, S["d_back"], S["s"])
+            S["e_su"].record(S["up"])
+        S["s"].wait_event(S["e_su"])
+        mb.decompress_into(S["ws"], S["d_s"], c, S["d_back"], S["s"])
+        S["e_dc"].record(S["s"])
+        S["down"].wait_event(S["e_dc"])
+        with torch.cuda.stream(S["down"]):
             S["h_out"].copy_(S["d_back"].view(torch.uint8), non_blocking=True)
+            S["e_free"].record(S["down"])
 
     cur = torch.cuda.current_stream()
     for it in range(1 + args.e2e_steps):  # (a)
@@ -498,8 +523,12 @@ def run_mans(args):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(cur)
+        for st_ in (sets[0]["up"], sets[0]["down"], sets[0]["s"]):
+            st_.wait_stream(cur)
         first_half(sets[0])
         second_half(sets[0])
+        for st_ in (sets[0]["up"], sets[0]["down"], sets[0]["s"]):
+            cur.wait_stream(st_)
         b.record(cur)
         torch.cuda.synchronize()
         if it > 0:
@@ -514,8 +543,8 @@ def run_mans(args):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(cur)
-        for S in sets:
-            S["s"].wait_stream(cur)
+        for st_ in [x for S in sets for x in (S["up"], S["down"], S["s"])]:
+            st_.wait_stream(cur)
         steps_here = n_pipe if timed else depth
         pending = []
         for k in range(steps_here):
@@ -526,8 +555,8 @@ def run_mans(args):
                 second_half(pending.pop(0))
         while pending:
             second_half(pending.pop(0))
-        for S in sets:
-            cur.wait_stream(S["s"])
+        for st_ in [x for S in sets for x in (S["up"], S["down"], S["s"])]:
+            cur.wait_stream(st_)
         b.record(cur)
         torch.cuda.synchronize()
     e2e_pipe_ms = a.elapsed_time(b) / n_pipe
@@ -574,7 +603,7 @@ def run_mans(args):
             "e2e": {"value": round(world * U / (e2e_step_ms / 1e3) / 1e9, 3), "unit": "GB/s",
                     "h2d_bytes_per_step": U + C, "d2h_bytes_per_step": 8 + C + U,
                     "ms_per_step": round(e2e_step_ms, 3),
-                    "mode": f"{n_pipe} buffers pipelined over {depth} streams with their own device buffers"},
+                    "mode": f"{n_pipe} buffers pipelined over {depth} buffer sets, each with upload, download and kernel streams"},
             "e2e_sequential": {"value": round(world * U / (e2e_seq_step_ms / 1e3) / 1e9, 3),
                                "unit": "GB/s", "ms_per_step": round(e2e_seq_step_ms, 3),
                                "mode": "one buffer at a time"},
