@@ -22,10 +22,8 @@ CPU uint32 mapping).
 from __future__ import annotations
 
 import argparse
-import glob
 import json
 import os
-import re
 import statistics
 import sys
 import threading
@@ -77,50 +75,16 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="override the element count (profiling runs)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--check-oracle", action="store_true",
-                    help="also compare the whole stream with the multi-threaded oracle")
+    ap.add_argument("--traffic-json", default=os.path.join(ROOT, "profiles", "dram_traffic.json"),
+                    help="ncu-measured DRAM bytes per launch of each kernel (roofline.traffic)")
+    ap.add_argument("--no-check-oracle", action="store_true",
+                    help="skip the comparison of the whole stream with the multi-threaded "
+                         "oracle (run after the timed region)")
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------- data
-def gen_device(workload: str, n: int, seed: int):
-    """Seeded synthetic input generated on the GPU (same distributions as
-    mans_b200.workloads, which makes the CPU samples)."""
-    import torch
-    g = torch.Generator(device="cuda")
-    g.manual_seed(seed)
-    chunk = 1 << 26
-    if workload == "detector_u32":
-        out = torch.empty(n, dtype=torch.int64, device="cuda")
-        for s in range(0, n, chunk):
-            m = min(chunk, n - s)
-            alpha = torch.full((m,), 0.5, device="cuda")
-            v = torch.round(torch._standard_gamma(alpha, generator=g) * 20.0).to(torch.int64)
-            peak = torch.rand(m, device="cuda", generator=g) < 0.001
-            pv = torch.randint(10_000, 1_000_001, (m,), device="cuda", generator=g)
-            out[s:s + m] = torch.where(peak, pv, v)
-        return out.to(torch.int32).view(torch.uint32)
-    if workload == "laplace_u16":
-        from mans_b200 import workloads as W
-        x = W.laplace_u16(n, seed)
-        return torch.from_numpy(x.view(np.uint8).copy()).cuda().view(torch.uint16)
-    if workload in ("gradient_u16", "quant_u32"):
-        it = {"elem": 2 if workload == "gradient_u16" else 4, "n": n, "off": 0, "a": 613.0, "b": -287.0}
-        it["bytes"] = n * it["elem"]
-        pool = gen_mixed_device([it], it["bytes"], seed)
-        return pool.view(torch.uint16 if it["elem"] == 2 else torch.uint32)
-    if workload == "volume_u16":
-        width = 2048
-        rows = n // width
-        out = torch.empty(n, dtype=torch.int32, device="cuda")
-        rs = 1 << 14
-        for r0 in range(0, rows, rs):
-            r = min(rs, rows - r0)
-            off = torch.randn(r, 1, device="cuda", generator=g) * 3000.0 + 20000.0
-            v = off + torch.randn(r, width, device="cuda", generator=g) * 150.0
-            out[r0 * width:(r0 + r) * width] = torch.clamp(torch.round(v), 0, 65535).to(torch.int32).view(-1)
-        return out.to(torch.int16).view(torch.uint16)
-    raise ValueError(workload)
+from mans_b200.workloads import gen_device, gen_mixed_device  # noqa: E402
 
 
 def gen_host_sample(workload: str, n: int, seed: int) -> np.ndarray:
@@ -209,16 +173,17 @@ def hbm_peak() -> tuple[float, str]:
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic(workload: str) -> dict:
-    """Per-launch DRAM bytes of each kernel from committed ncu summaries
-    (lines 'TRAFFIC <workload> <kernel> <bytes per launch>')."""
-    out = {}
-    for f in glob.glob(os.path.join(ROOT, "profiles", "*.txt")) + glob.glob(os.path.join(ROOT, "profiles", "*.md")):
-        for line in open(f, errors="ignore"):
-            m = re.match(r"^\s*TRAFFIC\s+(\S+)\s+(\S+)\s+(\d+)", line)
-            if m and m.group(1) == workload:
-                out[m.group(2)] = int(m.group(3))
-    return out
+def measured_traffic(path: str, workload: str, n: int) -> dict:
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum)
+    of each kernel, as measured by ncu on this workload at this size and
+    recorded in a JSON data file: {workload: {"n": elements, "kernels":
+    {kernel: bytes}}}. Empty when the file holds no record for (workload, n)."""
+    try:
+        with open(path) as f:
+            rec = json.load(f).get(workload, {})
+    except (OSError, ValueError):
+        return {}
+    return {k: int(v) for k, v in rec.get("kernels", {}).items()} if rec.get("n") == n else {}
 
 
 def reduce_max_over_ranks(values, dist=None, device="cuda"):
@@ -577,7 +542,7 @@ def run_mans(args):
                  "unmap": "adm_u32_unmap_kernel" if elem == 4 else "adm_u16_unmap_kernel"}
         dom = max(k_ms, key=lambda k: k_ms[k])
         achieved = algo[dom] / (k_ms[dom] / 1e3) / 1e9
-        traffic = ncu_traffic(args.workload).get(names[dom])
+        traffic = measured_traffic(args.traffic_json, args.workload, n).get(names[dom])
         kernels = {names[k]: {"ms": round(k_ms[k], 4), "algorithmic_bytes": algo[k],
                               "gbs": round(algo[k] / (k_ms[k] / 1e3) / 1e9, 1) if k_ms[k] else None,
                               "frac_of_hbm": round(algo[k] / (k_ms[k] / 1e3) / 1e9 / peak, 4) if k_ms[k] else None}
@@ -619,8 +584,14 @@ def run_mans(args):
             n_sample = {"detector_u32": 1 << 24, "laplace_u16": n, "volume_u16": 1 << 25,
                         "gradient_u16": 1 << 25, "quant_u32": 1 << 24}[args.workload]
             result["cpu_baseline"] = cpu_round_trip(args.workload, n_sample, reps=5, warm=2)
-        if args.check_oracle:
+        if not args.no_check_oracle:
+            t0 = time.time()
             result["oracle_stream_equal"] = check_oracle(args, x, out[:C])
+            result["oracle_check"] = {
+                "what": "the whole compressed stream of the benchmarked input, byte for byte, "
+                        "against the oracle's group- and block-parallel restatement "
+                        "(oracle/mans_oracle.c), after the timed region",
+                "seconds": round(time.time() - t0, 1)}
         print(json.dumps(result), flush=True)
 
 
@@ -642,29 +613,6 @@ def mixed_layout(count: int, seed: int = 3):
                       "a": float(ab[i, 0]), "b": float(ab[i, 1])})
         off += (nb + 255) // 256 * 256
     return items, off
-
-
-def gen_mixed_device(items, total: int, seed: int):
-    import torch
-    g = torch.Generator(device="cuda")
-    g.manual_seed(seed)
-    pool = torch.zeros(total, dtype=torch.uint8, device="cuda")
-    for it in items:
-        n = it["n"]
-        if it["elem"] == 2:
-            idx = torch.arange(n, device="cuda", dtype=torch.int64)
-            h = -(-n // 1024)
-            v = (8000.0 + it["a"] * (idx % 1024).to(torch.float32) / 1024.0
-                 + it["b"] * (idx // 1024).to(torch.float32) / h
-                 + torch.randn(n, device="cuda", generator=g) * 200.0)
-            v = torch.clamp(torch.round(v), 0, 65535).to(torch.int32).to(torch.int16)
-        else:
-            u = torch.rand(n, device="cuda", generator=g, dtype=torch.float64) - 0.5
-            lap = -300.0 * torch.sign(u) * torch.log(torch.clamp(1.0 - 2.0 * u.abs(), min=1e-300))
-            v = torch.clamp(torch.round(lap).to(torch.int64) + (1 << 31), 0, (1 << 32) - 1)
-            v = torch.where(v >= (1 << 31), v - (1 << 32), v).to(torch.int32)
-        pool[it["off"]:it["off"] + it["bytes"]].copy_(v.view(torch.uint8))
-    return pool
 
 
 def mixed_cpu_sample(reps: int, warm: int) -> dict:
@@ -1148,25 +1096,13 @@ def run_serve(args):
 
 
 def check_oracle(args, x, s) -> bool:
+    """The device stream s of input x equals the oracle's, byte for byte."""
     from oracle import pyoracle as O
     from tests.helpers import to_host
     xh = to_host(x, np.uint32 if x.element_size() == 4 else np.uint16)
-    sh = to_host(s)
-    if xh.dtype == np.uint32:
-        L = O.lib()
-        cap = L.mo_adm_u32_max_merged_size(xh.size)
-        m = np.empty(cap, np.uint8)
-        ms = L.mo_adm_u32_map_par(xh.ctypes.data_as(O.u32p), xh.size, m.ctypes.data_as(O.u8p), cap)
-        scap = O.max_compressed_size(ms)
-        ref = np.empty(scap, np.uint8)
-        scr = np.empty(L.mo_ans_par_scratch_words(ms), np.uint16)
-        sst = np.empty(32 * ((ms + 4095) // 4096), np.uint32)
-        snw = np.empty((ms + 4095) // 4096, np.uint32)
-        r = L.mo_ans_encode_par(args.precision, m.ctypes.data_as(O.u8p), ms, ref.ctypes.data_as(O.u8p),
-                                scap, scr.ctypes.data_as(O.u16p), sst.ctypes.data_as(O.u32p),
-                                snw.ctypes.data_as(O.u32p))
-        return bool(r == sh.size and np.array_equal(ref[:r], sh))
-    return bool(np.array_equal(O.compress(xh, args.precision), sh))
+    want = O.compress_par(xh, args.precision)
+    got = to_host(s)
+    return bool(got.size == want.size and np.array_equal(got, want))
 
 
 def main():

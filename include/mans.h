@@ -56,8 +56,10 @@ typedef struct mans_workspace mans_workspace;
  * Workspace: device scratch reused across calls, so a call allocates
  * nothing. max_input_bytes bounds the uncompressed size of one call;
  * merged_capacity bounds the mapped (ADM) bytes (0 = 2.1 x max_input_bytes,
- * which always suffices for MANS_U32 and MANS_U8). A workspace serves one
- * stream at a time.
+ * which always suffices for MANS_U32 and MANS_U8, and for MANS_U16 data whose
+ * values stay within a few thousand of their 512-element group's mean; pass
+ * mans_max_mapped_size(MANS_U16, n) to accept any uint16 input). A workspace
+ * serves one stream at a time.
  * ---------------------------------------------------------------------- */
 mans_status mans_workspace_create(mans_workspace** ws, uint64_t max_input_bytes,
                                   uint64_t merged_capacity);
@@ -79,8 +81,24 @@ mans_status mans_workspace_set_timing(mans_workspace* ws, int enable);
  * the recorded events, then clears the record. */
 mans_status mans_workspace_kernel_times(mans_workspace* ws, float ms[4], int calls[2]);
 
-/* Upper bound of the compressed size for n elements of dtype when the mapped
- * bytes fit the default workspace. */
+/* Worst-case mapped (ADM) bytes of n elements of dtype, in any layout, for
+ * any values. uint16: a lane's unary stream holds at most 16 x 521 bits
+ * (k <= ceil(65535/126)), so a 512-element group maps to at most 32 x 1,042
+ * bit bytes plus one code byte per element and its header fields -- about 33
+ * bytes per input byte for pathological data, against ~1.2 for smooth data.
+ * uint32: at most 8 record bytes per element plus 40 header bytes per group
+ * (~2.02 x the input). MANS_U8: n. Pass it as the workspace's
+ * merged_capacity to accept any uint16 input. */
+uint64_t mans_max_mapped_size(mans_dtype dtype, uint64_t n_elems);
+/* Worst-case rANS stream bytes for mapped_bytes of rANS input (32 lanes x 90
+ * words per 4 KiB block plus the header, pdf, states and block words). */
+uint64_t mans_stream_bound(uint64_t mapped_bytes);
+/* Upper bound of the compressed size for n elements of dtype, for any values:
+ * mans_stream_bound(min(mans_max_mapped_size(dtype, n), 0xfffffff0)). Mapped
+ * buffers beyond 0xfffffff0 bytes (the rANS header's u32 counts) are
+ * rejected, so the clamp keeps the bound valid for every stream that can
+ * exist. The data must also fit the workspace's merged_capacity (see
+ * mans_workspace_create) or the call reports MANS_ERR_WORKSPACE_OVERFLOW. */
 uint64_t mans_max_compressed_size(mans_dtype dtype, uint64_t n_elems);
 
 /* ------------------------------------------------------------------------
@@ -175,12 +193,23 @@ mans_status mans_ans_last_status(mans_stream_t stream, uint64_t* detail);
  * calls that overlap on the GPU race, so issue them on one stream. */
 mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_in, uint32_t in_size,
                                     uint8_t* d_out, uint32_t* d_out_size, mans_stream_t stream);
+/* The device-side status of the last mans_ans_encode_noalloc call on the
+ * current device (an expired bounded wait, a stream past its bound): waits
+ * for `stream`, then copies the status and *detail out of the fixed scratch
+ * array, allocating nothing. The next mans_ans_encode_noalloc call clears it,
+ * so read it before issuing the next call. MANS_OK when no call was made. */
+mans_status mans_ans_noalloc_status(mans_stream_t stream, uint64_t* detail);
 
 /* ------------------------------------------------------------------------
- * Self-describing frames: a 64-byte header (magic "MANS", version, element
- * type, layout, precision, element count, mapped and stream sizes; FORMAT.md
- * in the repository root documents every byte) in front of a MANS stream, so
- * a frame decodes with nothing kept out of band. The reference keeps the
+ * Self-describing frames: a 64-byte header in front of a MANS stream, so
+ * a frame decodes with nothing kept out of band. Header, little endian:
+ *   0 u32 magic 0x534e414d ("MANS")   4 u16 version (1)
+ *   6 u8 dtype (1, 2, 4)              7 u8 layout (0, 1, 2)
+ *   8 u8 precision (9..11)            9 u8 flags (0)
+ *  10 u16 header bytes (64)          12 u32 reserved (0)
+ *  16 u64 element count              24 u64 mapped bytes (the rANS input)
+ *  32 u64 stream bytes               40 24 reserved bytes (0)
+ * The reference keeps the
  * element count and type outside the stream (examples/compress.cu:79-97) and,
  * for uint32, writes no centers or lengths at all (mappingV9_fuse.cu:998);
  * the frame plus the record layout's header carry both.

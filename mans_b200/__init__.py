@@ -53,6 +53,8 @@ SIGNATURES = {
     "mans_workspace_set_timing": (_i32, [_vp, _i32]),
     "mans_workspace_kernel_times": (_i32, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "mans_max_compressed_size": (_u64, [_i32, _u64]),
+    "mans_max_mapped_size": (_u64, [_i32, _u64]),
+    "mans_stream_bound": (_u64, [_u64]),
     "mans_compress": (_i32, [_vp, _i32, _vp, _u64, _vp, _u64, _vp, _i32, _vp]),
     "mans_decompress": (_i32, [_vp, _i32, _vp, _u64, _vp, _u64, _vp]),
     "mans_compress_ex": (_i32, [_vp, _i32, _i32, _vp, _u64, _vp, _u64, _vp, _i32, _vp]),
@@ -70,6 +72,7 @@ SIGNATURES = {
     "mans_ans_max_compressed_size": (_u32, [_u32]),
     "mans_ans_last_status": (_i32, [_vp, C.POINTER(_u64)]),
     "mans_ans_encode_noalloc": (_i32, [_i32, _vp, _u32, _vp, _vp, _vp]),
+    "mans_ans_noalloc_status": (_i32, [_vp, C.POINTER(_u64)]),
     "mans_batch_create": (_i32, [C.POINTER(_vp), _u32, _u64, _u32]),
     "mans_batch_destroy": (_i32, [_vp]),
     "mans_batch_device_bytes": (_u64, [_vp]),
@@ -153,6 +156,16 @@ def dtype_code(t) -> int:
 
 def max_compressed_size(dtype: int, n_elems: int) -> int:
     return int(load().mans_max_compressed_size(dtype, n_elems))
+
+
+def max_mapped_size(dtype: int, n_elems: int) -> int:
+    """Worst-case mapped bytes of n elements (mans_max_mapped_size)."""
+    return int(load().mans_max_mapped_size(dtype, n_elems))
+
+
+def stream_bound(mapped_bytes: int) -> int:
+    """Worst-case stream bytes for mapped_bytes of rANS input (mans_stream_bound)."""
+    return int(load().mans_stream_bound(mapped_bytes))
 
 
 def getMaxCompressedSize(in_size: int) -> int:  # noqa: N802 (reference name)
@@ -318,11 +331,14 @@ FRAME_HEADER_BYTES = 64
 _CODE_DTYPE = {MANS_U8: "uint8", MANS_U16: "uint16", MANS_U32: "uint32"}
 
 
-def frame_parse(header: bytes) -> FrameInfo:
-    """Parse a frame header from host bytes (the whole frame, or at least its 64-byte header)."""
+def frame_parse(header: bytes, avail: Optional[int] = None) -> FrameInfo:
+    """Parse a frame header from host bytes (the whole frame, or at least its
+    64-byte header). avail: bytes of the frame available (default: len(header)
+    when more than the header is given, else unknown)."""
     buf = (C.c_uint8 * max(len(header), 1)).from_buffer_copy(bytes(header) or b"\0")
     info = FrameInfo()
-    avail = len(header) if len(header) > FRAME_HEADER_BYTES else (1 << 64) - 1
+    if avail is None:
+        avail = len(header) if len(header) > FRAME_HEADER_BYTES else (1 << 64) - 1
     _check(load().mans_frame_parse(C.cast(buf, C.c_void_p), avail, C.byref(info)), "mans_frame_parse")
     return info
 

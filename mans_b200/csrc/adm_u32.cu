@@ -59,11 +59,26 @@ __global__ __launch_bounds__(kUnmap32Threads) void adm_u32_unmap_kernel(
 }
 
 // ------------------------------------------------------------------------
+static int occupancy32(const void* fn, int threads, size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    n = 1;
+  }
+  return n > 0 ? n : 1;
+}
+
+// Called once per device (with the device current) by init_launch_cfg; the
+// results live in the caller's LaunchCfg, so launches on several devices or
+// from several host threads read no shared mutable state.
 void init_adm_u32_launch_cfg(LaunchCfg& cfg) {
   cudaFuncSetAttribute(adm_u32_map_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(Map32Smem));
   cudaFuncSetAttribute(adm_u32_unmap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(Unmap32Smem));
+  cfg.map32_ctas = occupancy32((const void*)adm_u32_map_kernel, kMap32Threads, sizeof(Map32Smem));
+  cfg.unmap32_ctas =
+      occupancy32((const void*)adm_u32_unmap_kernel, kUnmap32Threads, sizeof(Unmap32Smem));
 }
 
 static unsigned grid_for(uint64_t want, uint64_t cap) {
@@ -73,12 +88,7 @@ static unsigned grid_for(uint64_t want, uint64_t cap) {
 cudaError_t launch_adm_u32_map(const uint32_t* in, uint64_t n, uint8_t* m, uint64_t m_cap,
                                Ctrl* ctrl, unsigned long long* flags, int prob_bits,
                                const LaunchCfg& cfg, cudaStream_t s) {
-  static int occ = 0;
-  if (occ == 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adm_u32_map_kernel, kMap32Threads,
-                                                  sizeof(Map32Smem));
-    if (occ < 1) occ = 1;
-  }
+  const int occ = cfg.map32_ctas > 0 ? cfg.map32_ctas : 1;
   const uint64_t ctas = div_up_u64(div_up_u64(n, kAdmGroup), kMap32Warps);
   adm_u32_map_kernel<<<grid_for(ctas, (uint64_t)cfg.sms * occ), kMap32Threads, sizeof(Map32Smem),
                        s>>>(in, n, m, m_cap, ctrl, flags, prob_bits);
@@ -87,12 +97,7 @@ cudaError_t launch_adm_u32_map(const uint32_t* in, uint64_t n, uint8_t* m, uint6
 
 cudaError_t launch_adm_u32_unmap(const uint8_t* m, uint64_t n, uint32_t* out, Ctrl* ctrl,
                                  const LaunchCfg& cfg, cudaStream_t s) {
-  static int occ = 0;
-  if (occ == 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adm_u32_unmap_kernel, kUnmap32Threads,
-                                                  sizeof(Unmap32Smem));
-    if (occ < 1) occ = 1;
-  }
+  const int occ = cfg.unmap32_ctas > 0 ? cfg.unmap32_ctas : 1;
   const uint64_t groups = div_up_u64(n, kAdmGroup);
   adm_u32_unmap_kernel<<<grid_for(div_up_u64(groups, kUnmap32Warps), (uint64_t)cfg.sms * occ),
                          kUnmap32Threads, sizeof(Unmap32Smem), s>>>(m, n, out, ctrl);

@@ -95,3 +95,32 @@ extern "C" mans_status mans_ans_encode_noalloc(int precision, const uint8_t* d_i
                           precision, div_up_u64(in_size, kAnsBlock), cfg, s, nullptr);
   return e == cudaSuccess ? MANS_OK : MANS_ERR_CUDA;
 }
+
+// Device-side errors of the last call (an expired bounded wait, a block past
+// its word bound) land in the control block at the start of the fixed array;
+// this copies them out with a synchronous copy into caller stack memory, so it
+// allocates nothing either. The next encode call's memset clears them.
+extern "C" mans_status mans_ans_noalloc_status(mans_stream_t stream, uint64_t* detail) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return MANS_ERR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return MANS_ERR_INVALID_ARG;
+  unsigned char* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (g_state[dev].ready) scratch = g_state[dev].scratch;
+  }
+  if (detail) *detail = 0;
+  if (!scratch) return MANS_OK;  // no call has been made on this device
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  struct {
+    uint32_t status, pad;
+    unsigned long long detail;
+  } h = {0, 0, 0};
+  static_assert(offsetof(Ctrl, status) == 0 && offsetof(Ctrl, detail) == 8,
+                "status and detail lead the control block");
+  if (cudaMemcpy(&h, scratch, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return MANS_ERR_CUDA;
+  if (detail) *detail = h.detail;
+  return (mans_status)h.status;
+}

@@ -80,8 +80,16 @@ mans_status mans_frame_parse(const void* header, uint64_t avail, mans_frame_info
       f.precision < 9 || f.precision > 11 || f.n_elems > (~0ull) / eb)
     return MANS_ERR_BAD_STREAM;
   if (f.dtype == MANS_U8 && f.mapped_bytes != f.n_elems) return MANS_ERR_BAD_STREAM;
+  // The mapped bytes cannot exceed the worst case for the element count (nor
+  // the rANS header's u32 count), and the stream cannot exceed the worst case
+  // for the mapped bytes: this bounds every size handed to the decoder even
+  // when the frame's available size is unknown.
+  if (f.mapped_bytes > mans_max_mapped_size(f.dtype, f.n_elems) || f.mapped_bytes > 0xffffffffull)
+    return MANS_ERR_BAD_STREAM;
   if (f.stream_bytes < 544) return MANS_ERR_BAD_STREAM;  // header + pdf of an empty stream
-  if (avail != ~0ull && kFrameBytes + f.stream_bytes > avail) return MANS_ERR_BAD_STREAM;
+  if (f.stream_bytes > mans_stream_bound(f.mapped_bytes)) return MANS_ERR_BAD_STREAM;
+  // compared without an addition that could wrap
+  if (avail != ~0ull && f.stream_bytes > avail - kFrameBytes) return MANS_ERR_BAD_STREAM;
   *info = f;
   return MANS_OK;
 }

@@ -358,12 +358,30 @@ mans_status mans_workspace_status(mans_workspace* ws, mans_stream_t stream, uint
   return (mans_status)h.status;
 }
 
+uint64_t mans_max_mapped_size(mans_dtype dtype, uint64_t n_elems) {
+  // Beyond 2^40 elements every sum below could wrap; no such buffer exists.
+  if (elem_bytes(dtype) == 0 || n_elems > (1ull << 40)) return 0;
+  const uint64_t g = div_up_u64(n_elems, kAdmGroup);
+  switch (dtype) {
+    case MANS_U8: return n_elems;
+    case MANS_U16:
+      // lanes of at most 16 x 521 bits = 1,042 bytes, 32 lanes per group;
+      // codes; the largest header (CPU-V2: 6 bytes per group + 4)
+      return g * (32ull * kU16MaxLaneBytes + 6) + 4 + n_elems;
+    case MANS_U32:
+      // at most 8 record bytes per element; 40 header bytes per group
+      return 40 * g + 8 * n_elems;
+  }
+  return 0;
+}
+
+uint64_t mans_stream_bound(uint64_t mapped_bytes) { return ans_bound(mapped_bytes); }
+
 uint64_t mans_max_compressed_size(mans_dtype dtype, uint64_t n_elems) {
   const uint64_t eb = elem_bytes(dtype);
   if (eb == 0) return 0;
-  const uint64_t in_bytes = n_elems * eb;
-  if (dtype == MANS_U8) return ans_bound(in_bytes);
-  const uint64_t merged = in_bytes / 10 * 21 + 4096;
+  if (dtype == MANS_U8) return ans_bound(n_elems);
+  const uint64_t merged = mans_max_mapped_size(dtype, n_elems);
   return ans_bound(merged < kMaxMerged ? merged : kMaxMerged);
 }
 

@@ -33,6 +33,9 @@ __host__ __device__ constexpr uint64_t ans_overhead(uint64_t nb) {
 constexpr int kAdmChunk = 16;     // elements per lane
 constexpr int kAdmGroup = 512;    // elements per group (one warp)
 constexpr uint32_t kAdmStep = 126;
+// Longest uint16 lane stream in bytes: 16 elements of at most
+// ceil(65535 / 126) = 521 bits each.
+constexpr uint64_t kU16MaxLaneBytes = (kAdmChunk * 521 + 7) / 8;  // 1,042
 constexpr int kAdmGroupsPerTile = 8;  // warps (groups in flight) per CTA of the mappers
 // uint16 groups per unit of the map's claims and look-back (a uint16 group is
 // 1 KiB of input; two halve the per-byte cost of claims and look-backs).

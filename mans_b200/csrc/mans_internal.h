@@ -26,6 +26,8 @@ struct LaunchCfg {
   int enc_slot_ctas = 0;  // resident CTAs per SM of the encode kernel (global slots)
   int dec_ctas = 0;     // resident CTAs per SM of the decode kernel
   int map_ctas = 0;     // resident CTAs per SM of the ADM map kernels
+  int map32_ctas = 0;   // resident CTAs per SM of the uint32 ADM map kernel
+  int unmap32_ctas = 0; // resident CTAs per SM of the uint32 ADM unmap kernel
   int hist_ctas = 0;    // resident CTAs per SM of the byte histogram kernel
 };
 

@@ -881,6 +881,69 @@ int mo_ans_decode_par(const uint8_t* in, uint64_t in_size, uint8_t* out, uint64_
   return 0;
 }
 
+/* Group-parallel uint16 mapping (same bytes as mo_adm_u16_map_layout): pass 1
+ * computes every group's center and signal length, a serial scan gives the
+ * offsets, pass 2 writes each group's codes and lane streams. out == NULL
+ * returns the mapped size only. */
+int64_t mo_adm_u16_map_layout_par(const uint16_t* in, uint64_t n, int layout, uint8_t* out,
+                                  uint64_t cap) {
+  uint64_t g = div_up(n, ADM_GROUP);
+  if (layout < 0 || layout > 2) return -2;
+  uint32_t* len = (uint32_t*)calloc(g ? g : 1, sizeof(uint32_t));
+  uint32_t* ctr = (uint32_t*)calloc(g ? g : 1, sizeof(uint32_t));
+  uint64_t* excl = (uint64_t*)calloc(g ? g : 1, sizeof(uint64_t));
+#pragma omp parallel for schedule(static)
+  for (int64_t grp = 0; grp < (int64_t)g; ++grp)
+    len[grp] = adm_group_len_u16(in, n, (uint64_t)grp, &ctr[grp]);
+  uint64_t tot = 0;
+  for (uint64_t grp = 0; grp < g; ++grp) {
+    excl[grp] = tot;
+    tot += len[grp];
+  }
+  const uint64_t hdr = mo_adm_u16_header_bytes(n, layout);
+  const uint64_t msize = hdr + n + 32 * tot;
+  if (!out || msize > cap) {  /* out == NULL: size query */
+    free(len);
+    free(ctr);
+    free(excl);
+    return out ? -1 : (int64_t)msize;
+  }
+  const uint64_t pre = hdr - 2 * g;
+  uint8_t* p_len = out;
+  uint8_t* p_ctr = out + pre;
+  uint8_t* p_code = out + hdr;
+  uint8_t* p_bits = out + hdr + n;
+#pragma omp parallel
+  {
+    uint8_t lanebuf[ADM_U16_MAX_LANE_BYTES + 8];
+#pragma omp for schedule(static)
+    for (int64_t gi = 0; gi < (int64_t)g; ++gi) {
+      const uint64_t grp = (uint64_t)gi;
+      if (layout == MO_LAYOUT_V12) wr16(p_len + 2 * grp, (uint16_t)len[grp]);
+      else wr32(p_len + 4 * grp, (uint32_t)excl[grp]);
+      wr16(p_ctr + 2 * grp, (uint16_t)ctr[grp]);
+      const uint32_t L = len[grp];
+      for (int l = 0; l < ADM_LANES; ++l) {
+        uint64_t s, e;
+        lane_range(n, grp, l, &s, &e);
+        memset(lanebuf, 0, sizeof(lanebuf));
+        if (layout == MO_LAYOUT_V12 && s >= e) {
+          memset(lanebuf, 0xFF, L);
+        } else {
+          uint32_t b = adm_lane_bits_u16(in, s, e, ctr[grp], lanebuf, p_code + s);
+          if (b < L * 8) lanebuf[b >> 3] |= (uint8_t)(0xFFu >> (b & 7));
+        }
+        memcpy(p_bits + 32 * excl[grp] + (uint64_t)l * L, lanebuf, L);
+      }
+    }
+  }
+  if (layout == MO_LAYOUT_CPUV2) wr32(p_len + 4 * g, (uint32_t)tot);
+  free(len);
+  free(ctr);
+  free(excl);
+  return (int64_t)msize;
+}
+
 /* Group-parallel uint32 mapping: pass 1 sizes every group's records, a
  * serial scan gives offsets, pass 2 writes. */
 int64_t mo_adm_u32_map_par(const uint32_t* in, uint64_t n, uint8_t* out, uint64_t cap) {

@@ -78,6 +78,8 @@ int64_t mo_ans_encode_par(int prob_bits, const uint8_t* in, uint64_t n, uint8_t*
                           uint64_t cap, uint16_t* scratch, uint32_t* scratch_states,
                           uint32_t* scratch_nw);
 int mo_ans_decode_par(const uint8_t* in, uint64_t in_size, uint8_t* out, uint64_t out_cap);
+int64_t mo_adm_u16_map_layout_par(const uint16_t* in, uint64_t n, int layout, uint8_t* out,
+                                  uint64_t cap);
 int64_t mo_adm_u32_map_par(const uint32_t* in, uint64_t n, uint8_t* out, uint64_t cap);
 int mo_adm_u32_unmap_par(const uint8_t* m, uint64_t msize, uint64_t n, uint32_t* out);
 

@@ -71,6 +71,7 @@ def lib() -> C.CDLL:
             "mo_ans_par_scratch_words": (u64, [u64]),
             "mo_ans_encode_par": (i64, [i32, u8p, u64, u8p, u64, u16p, u32p, u32p]),
             "mo_ans_decode_par": (i32, [u8p, u64, u8p, u64]),
+            "mo_adm_u16_map_layout_par": (i64, [u16p, u64, i32, u8p, u64]),
             "mo_adm_u32_map_par": (i64, [u32p, u64, u8p, u64]),
             "mo_adm_u32_unmap_par": (i32, [u8p, u64, u64, u32p]),
         }
@@ -197,6 +198,41 @@ def decompress(s: np.ndarray, n: int, dtype, layout: int = LAYOUT_V15) -> np.nda
     if np.dtype(dtype) == np.uint16:
         return adm_u16_unmap(m, n, layout)
     return adm_u32_unmap(m, n)
+
+
+def compress_par(x: np.ndarray, prob_bits: int = 10, layout: int = LAYOUT_V15,
+                 threads: int = 0) -> np.ndarray:
+    """compress() with the group- and block-parallel (OpenMP) variants: the
+    same bytes, fast enough for inputs of several GiB."""
+    L = lib()
+    if threads:
+        L.mo_set_threads(threads)
+    n = x.size
+    if x.dtype == np.uint16:
+        x = np.ascontiguousarray(x)
+        cap = L.mo_adm_u16_map_layout_par(_ptr(x, u16p), n, layout, None, 0)
+        m = np.empty(max(cap, 1), np.uint8)
+        ms = L.mo_adm_u16_map_layout_par(_ptr(x, u16p), n, layout, _ptr(m), cap)
+    elif x.dtype == np.uint32:
+        x = np.ascontiguousarray(x)
+        cap = L.mo_adm_u32_max_merged_size(n)
+        m = np.empty(max(cap, 1), np.uint8)
+        ms = L.mo_adm_u32_map_par(_ptr(x, u32p), n, _ptr(m), cap)
+    else:
+        raise TypeError(x.dtype)
+    if ms < 0:
+        raise ValueError(f"mapping failed: {ms}")
+    scap = max_compressed_size(ms)
+    out = np.empty(scap, np.uint8)
+    nb = (ms + 4095) // 4096
+    scr = np.empty(max(L.mo_ans_par_scratch_words(ms), 1), np.uint16)
+    sst = np.empty(max(32 * nb, 1), np.uint32)
+    snw = np.empty(max(nb, 1), np.uint32)
+    r = L.mo_ans_encode_par(prob_bits, _ptr(m), ms, _ptr(out), scap, _ptr(scr, u16p),
+                            _ptr(sst, u32p), _ptr(snw, u32p))
+    if r < 0:
+        raise ValueError(f"ans_encode_par failed: {r}")
+    return out[:r]
 
 
 # ---------------------------------------------------------------- reference CPU ADM

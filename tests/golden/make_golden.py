@@ -298,4 +298,6 @@ if __name__ == "__main__":
             i = args.index("--only")
             only = tuple(args[i + 1].split(","))
             args = args[:i] + args[i + 2:]
-        main(args[0] if args else os.path.join(ROOT, "gpurun_out", "golden"), only)
+        if not args:
+            sys.exit("usage: make_golden.py OUTDIR [--only kinds] | --merge OUTDIR")
+        main(args[0], only)

@@ -54,8 +54,35 @@ def test_host_side_argument_checks():
 def test_max_compressed_size_is_a_bound(n, oracle):
     assert mb.getMaxCompressedSize(n) >= oracle.max_compressed_size(n)
     assert mb.max_compressed_size(mb.MANS_U8, n) >= oracle.max_compressed_size(n)
-    # uint16: the default workspace admits 2.1x the input bytes of mapped data
-    assert mb.max_compressed_size(mb.MANS_U16, n) >= oracle.max_compressed_size(int(2 * n * 2.1))
+    for dt in (mb.MANS_U16, mb.MANS_U32):
+        m = min(mb.max_mapped_size(dt, n), 0xFFFFFFF0)
+        assert mb.max_compressed_size(dt, n) == mb.stream_bound(m) >= oracle.max_compressed_size(m)
+
+
+def _wide_u16_patterns(n):
+    """uint16 inputs that map to the most bytes: alternating extremes, one
+    lane of 65535 per group over zeros (and the reverse), uniform noise."""
+    rng = np.random.default_rng(5)
+    one_lane = np.zeros(n, np.uint16)
+    one_lane.reshape(-1, 512)[:, :16] = 65535
+    return [np.tile(np.array([0, 65535], np.uint16), n // 2), one_lane, 65535 - one_lane,
+            rng.integers(0, 65536, n, dtype=np.uint16)]
+
+
+@pytest.mark.parametrize("n", [512, 8192, 65_536])
+def test_max_mapped_size_covers_the_widest_uint16_data(n, oracle):
+    """The worst-case bounds hold for the uint16 inputs that map widest (up to
+    about 65 mapped bytes per element) in every layout, and for uint32 data
+    of only escapes and of only 8-byte elements."""
+    for x in _wide_u16_patterns(n):
+        for layout in (0, 1, 2):
+            m = oracle.adm_u16_map(x, layout)
+            assert m.size <= mb.max_mapped_size(mb.MANS_U16, n)
+        assert oracle.compress(x, 9).size <= mb.max_compressed_size(mb.MANS_U16, n)
+    for x in (np.tile(np.array([0, 1 << 31], np.uint32), n // 2),
+              np.tile(np.array([0, 8 * 126 * 2], np.uint32), n // 2)):
+        assert oracle.adm_u32_map(x).size <= mb.max_mapped_size(mb.MANS_U32, n)
+        assert oracle.compress(x, 9).size <= mb.max_compressed_size(mb.MANS_U32, n)
 
 
 def test_division_table_is_exact():

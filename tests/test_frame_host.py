@@ -33,3 +33,26 @@ def test_frame_parse_checks_the_available_size():
     with pytest.raises(mb.MansError):
         mb.frame_parse(header(stream=701) + bytes(700))
     mb.frame_parse(header(stream=701))  # header alone: size unknown, accepted
+
+
+@pytest.mark.parametrize("stream", [2 ** 64 - 1, 2 ** 64 - 63, 2 ** 64 - 64, 2 ** 63])
+def test_frame_parse_rejects_wrapping_stream_sizes(stream):
+    """A stream size near 2^64 must not wrap the available-size check, and a
+    stream larger than any stream of its mapped bytes is rejected even when
+    the available size is unknown."""
+    for avail in (64 + 700, 2 ** 64 - 2, None):
+        with pytest.raises(mb.MansError) as e:
+            blob = header(stream=stream) + bytes(700)
+            mb.frame_parse(blob) if avail is None else mb.frame_parse(blob, avail)
+        assert e.value.code == 7
+
+
+def test_frame_parse_bounds_sizes_by_the_element_count():
+    # mapped bytes beyond the worst case of 1000 uint16 values
+    with pytest.raises(mb.MansError):
+        mb.frame_parse(header(mapped=mb.max_mapped_size(mb.MANS_U16, 1000) + 1))
+    # a stream beyond the worst case of its mapped bytes
+    with pytest.raises(mb.MansError):
+        mb.frame_parse(header(mapped=1200, stream=mb.stream_bound(1200) + 16))
+    f = mb.frame_parse(header(mapped=1200, stream=mb.stream_bound(1200)))
+    assert f.stream_bytes == mb.stream_bound(1200)

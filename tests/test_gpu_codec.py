@@ -214,6 +214,34 @@ def test_workspace_overflow_reports_status(torch_cuda, oracle):
     small.close()
 
 
+def test_worst_case_bounds_size_the_widest_uint16_data(torch_cuda, oracle):
+    """Sized only by the library's worst-case bounds -- mans_max_mapped_size
+    for the workspace's mapped capacity, mans_max_compressed_size for the
+    output -- the widest uint16 data (alternating 0 / 65535, about 65 mapped
+    bytes per element; one lane of 65535 per group over zeros) compresses to
+    the oracle's stream and decodes back."""
+    import torch
+    n = 65_536
+    one_lane = np.zeros(n, np.uint16)
+    one_lane.reshape(-1, 512)[:, :16] = 65535
+    for x in (np.tile(np.array([0, 65535], np.uint16), n // 2), one_lane):
+        w = mb.Workspace(2 * n, merged_capacity=mb.max_mapped_size(mb.MANS_U16, n))
+        out = torch.empty(mb.max_compressed_size(mb.MANS_U16, n), dtype=torch.uint8, device="cuda")
+        size = torch.zeros(1, dtype=torch.int64, device="cuda")
+        d = to_dev(x)
+        mb.compress_into(w, d, out, size, 10)
+        w.check(None, "compress")
+        got = to_host(out[: int(size.item())])
+        want = oracle.compress(x, 10)
+        assert oracle.adm_u16_map(x).size > 2.1 * 2 * n  # beyond the default workspace
+        np.testing.assert_array_equal(got, want)
+        back = torch.empty_like(d)
+        mb.decompress_into(w, out, got.size, back)
+        w.check(None, "decompress")
+        np.testing.assert_array_equal(to_host(back, np.uint16), x)
+        w.close()
+
+
 def test_repeated_calls_identical(ws):
     x = W.detector_u32(200_000, 8)
     a = gpu_compress(ws, x, 10)
