@@ -63,8 +63,11 @@ __global__ __launch_bounds__(kHistThreads) void hist_bytes_kernel(const uint8_t*
 // claimed one at a time (a claim held while another block is encoded would
 // stall every later block's look-back).
 // ------------------------------------------------------------------------
+// Five CTAs of eight warps per SM (40 warps; 48 registers a thread).
+constexpr int kEncMinCtas = 5;
+
 template <bool kSlots, bool kWide>
-__global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
+__global__ __launch_bounds__(kEncThreads, kEncMinCtas) void ans_encode_kernel(
     const uint8_t* __restrict__ in, uint8_t* __restrict__ out, uint64_t out_cap,
     unsigned long long* out_size64, uint32_t* out_size32, Ctrl* ctrl,
     unsigned long long* flags, int p, uint8_t* __restrict__ slots) {
@@ -123,26 +126,60 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
     }
   }
 
-  uint16_t* sout;
-  if constexpr (kSlots) {
-    sout = reinterpret_cast<uint16_t*>(slots + ((uint64_t)blockIdx.x * kEncWarps + warp) * kEncSlotBytes);
-  } else {
-    sout = reinterpret_cast<EncSmem*>(smem_raw)->out[warp];
-  }
   const uint32_t ahead = gridDim.x * kEncWarps;
-  while (!failed) {
-    const uint32_t b = warp_claim(&ctrl->tile_counter[1], lane);
-    if (b >= nb) break;
-    if (lane == 0 && (uint64_t)b + ahead < nb) {
-      const uint64_t s1 = ((uint64_t)b + ahead) * kAnsBlock;
-      prefetch_l2(in + s1, (uint32_t)min_u64(kAnsBlock, n - s1));
+  if constexpr (kSlots) {
+    // Two word slots per warp. A block's words wait in one slot for its
+    // stream offset while the warp encodes its next block into the other;
+    // the look-back of the waiting block then runs after that next block's
+    // aggregate is published, when its predecessors have usually finished,
+    // instead of stalling the warp. Every claimed block publishes its
+    // aggregate as soon as it is encoded, before any wait, so the deferred
+    // look-backs always complete.
+    uint16_t* const slot0 = reinterpret_cast<uint16_t*>(
+        slots + ((uint64_t)blockIdx.x * kEncWarps + warp) * 2 * kEncSlotBytes);
+    EncPending pend{0xffffffffu, 0, 0, nullptr};
+    uint32_t cur = 0;
+    while (!failed) {
+      const uint32_t b = warp_claim(&ctrl->tile_counter[1], lane);
+      if (b >= nb) break;
+      if (lane == 0 && (uint64_t)b + ahead < nb) {
+        const uint64_t s1 = ((uint64_t)b + ahead) * kAnsBlock;
+        prefetch_l2(in + s1, (uint32_t)min_u64(kAnsBlock, n - s1));
+      }
+      uint16_t* const sout = slot0 + cur * (kEncSlotBytes / 2);
+      uint32_t x;
+      uint32_t nw;
+      if constexpr (kWide)
+        nw = encode_words(in, n, b, ss.table4, ss.in[warp], bar, parity, sout, p, sink, lane, x);
+      else
+        nw = encode_words(in, n, b, ss.table2, ss.in[warp], bar, parity, sout, p, sink, lane, x);
+      if (lane == 0)
+        st_flag(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, (nw + 7) & ~7u));
+      if (pend.b != 0xffffffffu)
+        encode_finish<true>(out, out_cap, n, out_size64, out_size32, ctrl->pdf, flags, epoch, p,
+                            sink, pend, lane);
+      pend = EncPending{b, nw, x, sout};
+      cur ^= 1u;
     }
-    if constexpr (kWide)
-      encode_block<kSlots>(in, n, out, out_cap, out_size64, out_size32, ctrl->pdf, flags, epoch,
-                           p, sink, ss.table4, ss.in[warp], bar, parity, sout, b, lane);
-    else
-      encode_block<kSlots>(in, n, out, out_cap, out_size64, out_size32, ctrl->pdf, flags, epoch,
-                           p, sink, ss.table2, ss.in[warp], bar, parity, sout, b, lane);
+    if (pend.b != 0xffffffffu)
+      encode_finish<true>(out, out_cap, n, out_size64, out_size32, ctrl->pdf, flags, epoch, p,
+                          sink, pend, lane);
+  } else {
+    uint16_t* sout = reinterpret_cast<EncSmem*>(smem_raw)->out[warp];
+    while (!failed) {
+      const uint32_t b = warp_claim(&ctrl->tile_counter[1], lane);
+      if (b >= nb) break;
+      if (lane == 0 && (uint64_t)b + ahead < nb) {
+        const uint64_t s1 = ((uint64_t)b + ahead) * kAnsBlock;
+        prefetch_l2(in + s1, (uint32_t)min_u64(kAnsBlock, n - s1));
+      }
+      if constexpr (kWide)
+        encode_block<false>(in, n, out, out_cap, out_size64, out_size32, ctrl->pdf, flags, epoch,
+                            p, sink, ss.table4, ss.in[warp], bar, parity, sout, b, lane);
+      else
+        encode_block<false>(in, n, out, out_cap, out_size64, out_size32, ctrl->pdf, flags, epoch,
+                            p, sink, ss.table2, ss.in[warp], bar, parity, sout, b, lane);
+    }
   }
 
   __syncthreads();
@@ -161,18 +198,20 @@ __global__ __launch_bounds__(kEncThreads) void ans_encode_kernel(
 // ------------------------------------------------------------------------
 // Decode: one warp per block, decoded from its last step to its first. The
 // block's words are staged in shared memory with one bulk copy (read
-// backwards, data-dependently, every step); decoded bytes go straight to
-// global memory, 32 consecutive bytes per step. The next block is claimed
-// early and its words prefetched into L2 (no look-back: claiming ahead costs
-// nothing here).
+// backwards, data-dependently, every step); decoded bytes collect in a
+// 512-byte per-warp stage and leave as 16-byte stores every 16 steps. The
+// next block is claimed early and its words prefetched into L2 (no
+// look-back: claiming ahead costs nothing here).
 // ------------------------------------------------------------------------
 struct DecSmem {
-  uint32_t lut[1 << kMaxProbBits];
-  alignas(16) uint16_t in[kDecWarps][kEncOutWords];
+  uint32_t lut[1 << kMaxProbBits];  // below every warp's stage (see decode_full_smem)
+  DecWarpSmem warp[kDecWarps];
   uint64_t bar[kDecWarps];
 };
+// Five CTAs of eight warps per SM (40 warps): 45 KiB of shared memory each.
+constexpr int kDecMinCtas = 5;
 
-__global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
+__global__ __launch_bounds__(kDecThreads, kDecMinCtas) void ans_decode_kernel(
     const uint8_t* __restrict__ in, uint64_t in_size, uint8_t* __restrict__ out, uint64_t out_cap,
     Ctrl* ctrl, int expect_p, int record) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -223,7 +262,7 @@ __global__ __launch_bounds__(kDecThreads) void ans_decode_kernel(
         const uint32_t wn = ((bn.x & 0xffffu) + 7) & ~7u;
         if ((uint64_t)bn.y + wn <= cw) prefetch_l2(in + over + 2ull * bn.y, 2 * wn);
       }
-      decode_block(in, nb, n, cw, p, out, sm.lut, sm.in[warp], bar, parity, sink, b, lane);
+      decode_block(in, nb, n, cw, p, out, sm.lut, &sm.warp[warp], bar, parity, sink, b, lane);
       b = nxt;
     }
   }
@@ -280,7 +319,7 @@ cudaError_t launch_hist_bytes(const uint8_t* in, uint64_t n, Ctrl* ctrl, int pro
 }
 
 uint64_t ans_encode_slot_bytes(const LaunchCfg& cfg) {
-  return (uint64_t)cfg.sms * cfg.enc_slot_ctas * kEncWarps * kEncSlotBytes;
+  return (uint64_t)cfg.sms * cfg.enc_slot_ctas * kEncWarps * 2 * kEncSlotBytes;  // two per warp
 }
 
 cudaError_t launch_ans_encode(const uint8_t* in, uint8_t* out, uint64_t out_cap,

@@ -20,15 +20,17 @@ constexpr uint32_t kEncSlotBytes = (kEncOutWords * 2 + 127) / 128 * 128;
 constexpr uint32_t kEncStageBytes = kAnsBlock + 16;  // a block plus its 16-byte phase
 
 // The encoder's per-symbol entry in shared memory, expanded from the packed
-// table (make_enc_entry) so that a step needs no field extraction:
-// {reciprocal, renormalisation threshold pdf << (31 - p), bias, cmpl | shift << 16}.
-struct EncEntry4 {
+// table (make_enc_entry) so that a step needs almost no field extraction:
+// {reciprocal, renormalisation threshold pdf << (31 - p), bias,
+//  shift | cmpl << 5}. The quotient's shift is taken from the low five bits
+// of the last word by a wrapping funnel shift.
+struct alignas(16) EncEntry4 {
   uint32_t rcp, thr, bias, cs;
 };
 __device__ __forceinline__ EncEntry4 expand_enc_entry(uint2 e, int p) {
   const uint32_t cmpl = (e.y >> 13) & 0xfffu;
   return EncEntry4{e.x, ((1u << p) - cmpl) << (kAnsStateBits - p), e.y & 0x1fffu,
-                   cmpl | ((e.y >> 25) << 16)};
+                   (e.y >> 25) | (cmpl << 5)};
 }
 
 struct EncSmemSlots {  // words go to global slots
@@ -49,39 +51,37 @@ struct EncSmem {  // words compacted in shared memory
   alignas(16) uint16_t out[kEncWarps][kEncOutWords];
 };
 
-// One interleaved step: renormalise (emit 16 bits, lanes in ascending order
-// into the compacted word buffer), then x = (x/pdf << p) + x%pdf + cdf.
-// kGuard: drop words past the buffer (see encode_words).
-template <bool kGuard = false>
-__device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
-                                         const uint2* __restrict__ tab, uint16_t* __restrict__ out,
-                                         uint32_t& nw, uint32_t mp, uint32_t sh, uint32_t ltmask) {
-  const uint2 e = tab[sym];
+// The coding step's symbol arithmetic for precision kP:
+// x' = (xr / pdf << p) + xr % pdf + cdf = xr + bias + q * cmpl, q = xr / pdf.
+template <int kP>
+__device__ __forceinline__ uint32_t enc_code(uint32_t xr, const uint2& e) {
   const uint32_t cmpl = (e.y >> 13) & 0xfffu;
-  const uint32_t thr = (mp - cmpl) << sh;
-  const bool wr = valid && x >= thr;
-  const uint32_t vote = __ballot_sync(0xffffffffu, wr);
-  if (wr) {
-    const uint32_t idx = nw + __popc(vote & ltmask);
-    if (!kGuard || idx < kEncOutWords) out[idx] = (uint16_t)(x & 0xffffu);
-  }
-  nw += __popc(vote);
-  const uint32_t xr = wr ? (x >> 16) : x;
-  if (valid) {
-    const uint32_t q = __umulhi(xr, e.x) >> (e.y >> 25);
-    x = xr + (e.y & 0x1fffu) + q * cmpl;
-  } else {
-    x = xr;
-  }
+  const uint32_t q = __umulhi(xr, e.x) >> (e.y >> 25);
+  return xr + (e.y & 0x1fffu) + q * cmpl;
 }
-// The same step on an expanded entry (fewer integer operations per symbol).
-template <bool kGuard = false>
+template <int kP>
+__device__ __forceinline__ uint32_t enc_code(uint32_t xr, const EncEntry4& e) {
+  const uint32_t q = __funnelshift_r(__umulhi(xr, e.rcp), 0u, e.cs);  // shift = cs & 31
+  return xr + e.bias + q * (e.cs >> 5);
+}
+template <int kP>
+__device__ __forceinline__ uint32_t enc_threshold(const uint2& e) {
+  return ((1u << kP) - ((e.y >> 13) & 0xfffu)) << (kAnsStateBits - kP);
+}
+template <int kP>
+__device__ __forceinline__ uint32_t enc_threshold(const EncEntry4& e) {
+  return e.thr;
+}
+
+// One interleaved step: renormalise (emit 16 bits, lanes in ascending order
+// into the compacted word buffer), then code the symbol.
+// kGuard: drop words past the buffer (see encode_words).
+template <int kP, bool kGuard, typename TabT>
 __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
-                                         const EncEntry4* __restrict__ tab,
-                                         uint16_t* __restrict__ out, uint32_t& nw, uint32_t,
-                                         uint32_t, uint32_t ltmask) {
-  const EncEntry4 e = tab[sym];
-  const bool wr = valid && x >= e.thr;
+                                         const TabT* __restrict__ tab, uint16_t* __restrict__ out,
+                                         uint32_t& nw, uint32_t ltmask) {
+  const TabT e = tab[sym];
+  const bool wr = valid && x >= enc_threshold<kP>(e);
   const uint32_t vote = __ballot_sync(0xffffffffu, wr);
   if (wr) {
     const uint32_t idx = nw + __popc(vote & ltmask);
@@ -89,45 +89,21 @@ __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
   }
   nw += __popc(vote);
   const uint32_t xr = wr ? (x >> 16) : x;
-  if (valid) {
-    const uint32_t q = __umulhi(xr, e.rcp) >> (e.cs >> 16);
-    x = xr + e.bias + q * (e.cs & 0xffffu);
-  } else {
-    x = xr;
-  }
+  x = valid ? enc_code<kP>(xr, e) : xr;
 }
 
 __device__ __forceinline__ void discard_l2_line(const void* p) {
   asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
 }
 
-// Encode block b of one buffer (one warp) into the warp's word buffer sout
-// (with kSlots a per-warp slot in global memory, which stays in L2, else
-// shared memory): one bulk copy of the block into the warp's stage, then the
-// interleaved coding with symbols read eight steps ahead; the word count is
-// padded to a 16-byte multiple with zeros (GpuANSEncode.h:275). Returns the
-// number of words; x receives the lane's final state.
-template <typename TabT>
-__device__ __forceinline__ uint32_t encode_words(const uint8_t* __restrict__ in, uint64_t n,
-                                                 uint32_t b, const TabT* table, uint8_t* stage,
-                                                 uint64_t* bar, uint32_t& parity, uint16_t* sout,
-                                                 int p, const Sink& sink, int lane, uint32_t& x) {
+// The coding of one staged block (syms: the lane's first symbol in the stage,
+// bs bytes) at precision kP, symbols read eight steps ahead. Returns the word
+// count; x receives the lane's final state.
+template <int kP, typename TabT>
+__device__ __forceinline__ uint32_t encode_staged(const uint8_t* syms, uint32_t bs,
+                                                  const TabT* table, uint16_t* sout, int lane,
+                                                  uint32_t& x) {
   const uint32_t ltmask = lanemask_lt();
-  const uint32_t mp = 1u << p, sh = kAnsStateBits - p;
-  const uint64_t start = (uint64_t)b * kAnsBlock;
-  const uint32_t bs = (uint32_t)min_u64(kAnsBlock, n - start);
-  // one bulk copy of the block (rounded out to 16-byte boundaries) into this
-  // warp's stage; the previous block's reads of the stage are complete
-  __syncwarp();
-  if (lane == 0) {
-    const uintptr_t a0 = reinterpret_cast<uintptr_t>(in + start) & ~uintptr_t(15);
-    const uintptr_t a1 = (reinterpret_cast<uintptr_t>(in + start) + bs + 15) & ~uintptr_t(15);
-    bulk_load(stage, reinterpret_cast<const void*>(a0), (uint32_t)(a1 - a0), bar);
-  }
-  if (!mbar_wait(bar, parity) && lane == 0) report(sink, MANS_ERR_TIMEOUT, b);
-  parity ^= 1u;
-  const uint8_t* syms = stage + phase16(in + start) + lane;
-
   x = kAnsStartState;
   uint32_t nw = 0;
   const uint32_t full = bs >> 5;
@@ -144,27 +120,58 @@ __device__ __forceinline__ uint32_t encode_words(const uint8_t* __restrict__ in,
 #pragma unroll
       for (int u = 0; u < 8; ++u) nx[u] = syms[(j + 8 + u) * 32];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
+      for (int u = 0; u < 8; ++u) enc_step<kP, false>(true, x, cur[u], table, sout, nw, ltmask);
 #pragma unroll
       for (int u = 0; u < 8; ++u) cur[u] = nx[u];
     }
     if (nw <= kRoom) {
 #pragma unroll
-      for (int u = 0; u < 8; ++u) enc_step(true, x, cur[u], table, sout, nw, mp, sh, ltmask);
+      for (int u = 0; u < 8; ++u) enc_step<kP, false>(true, x, cur[u], table, sout, nw, ltmask);
       j += 8;
     }
   }
   const bool tail_valid = (uint32_t)lane < (bs & 31);
   if (nw <= kRoom && full - j <= 7) {  // at most eight more steps
-    for (; j < full; ++j) enc_step(true, x, syms[j * 32], table, sout, nw, mp, sh, ltmask);
+    for (; j < full; ++j) enc_step<kP, false>(true, x, syms[j * 32], table, sout, nw, ltmask);
     if (bs & 31)
-      enc_step(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw, mp, sh, ltmask);
+      enc_step<kP, false>(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw, ltmask);
   } else {
-    for (; j < full; ++j)
-      enc_step<true>(true, x, syms[j * 32], table, sout, nw, mp, sh, ltmask);
+    for (; j < full; ++j) enc_step<kP, true>(true, x, syms[j * 32], table, sout, nw, ltmask);
     if (bs & 31)
-      enc_step<true>(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw, mp, sh,
-                     ltmask);
+      enc_step<kP, true>(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw, ltmask);
+  }
+  return nw;
+}
+
+// Encode block b of one buffer (one warp) into the warp's word buffer sout
+// (with kSlots a per-warp slot in global memory, which stays in L2, else
+// shared memory): one bulk copy of the block into the warp's stage, then the
+// interleaved coding; the word count is padded to a 16-byte multiple with
+// zeros (GpuANSEncode.h:275). Returns the number of words; x receives the
+// lane's final state.
+template <typename TabT>
+__device__ __forceinline__ uint32_t encode_words(const uint8_t* __restrict__ in, uint64_t n,
+                                                 uint32_t b, const TabT* table, uint8_t* stage,
+                                                 uint64_t* bar, uint32_t& parity, uint16_t* sout,
+                                                 int p, const Sink& sink, int lane, uint32_t& x) {
+  const uint64_t start = (uint64_t)b * kAnsBlock;
+  const uint32_t bs = (uint32_t)min_u64(kAnsBlock, n - start);
+  // one bulk copy of the block (rounded out to 16-byte boundaries) into this
+  // warp's stage; the previous block's reads of the stage are complete
+  __syncwarp();
+  if (lane == 0) {
+    const uintptr_t a0 = reinterpret_cast<uintptr_t>(in + start) & ~uintptr_t(15);
+    const uintptr_t a1 = (reinterpret_cast<uintptr_t>(in + start) + bs + 15) & ~uintptr_t(15);
+    bulk_load(stage, reinterpret_cast<const void*>(a0), (uint32_t)(a1 - a0), bar);
+  }
+  if (!mbar_wait(bar, parity) && lane == 0) report(sink, MANS_ERR_TIMEOUT, b);
+  parity ^= 1u;
+  const uint8_t* syms = stage + phase16(in + start) + lane;
+  uint32_t nw;
+  switch (p) {
+    case 9: nw = encode_staged<9>(syms, bs, table, sout, lane, x); break;
+    case 10: nw = encode_staged<10>(syms, bs, table, sout, lane, x); break;
+    default: nw = encode_staged<11>(syms, bs, table, sout, lane, x); break;
   }
   // A table that fits the block's bytes keeps each lane within its bound of
   // words (kAnsMaxBlockWords / 32); only a table built from other bytes (two
@@ -237,7 +244,34 @@ __device__ __forceinline__ void encode_store(uint8_t* __restrict__ out, uint64_t
   }
 }
 
-// One block as the unit of the single-pass prefix (flags per block).
+// A block whose words wait in their slot for the block's stream offset.
+struct EncPending {
+  uint32_t b;      // block index (0xffffffff: none)
+  uint32_t nw;     // its words
+  uint32_t x;      // the lane's final state
+  uint16_t* sout;  // its word slot
+};
+
+// The second half of a block: the exclusive word prefix from the decoupled
+// look-back, the block's inclusive prefix, and the store.
+template <bool kSlots>
+__device__ __forceinline__ void encode_finish(
+    uint8_t* __restrict__ out, uint64_t out_cap, uint64_t n, unsigned long long* out_size64,
+    uint32_t* out_size32, const uint32_t* __restrict__ pdf, unsigned long long* flags,
+    uint32_t epoch, int p, const Sink& sink, const EncPending& pb, int lane) {
+  const uint32_t padded = (pb.nw + 7) & ~7u;
+  uint32_t prefix = 0;
+  if (pb.b > 0) {
+    prefix = lookback_exclusive(flags, pb.b, epoch, sink);
+    if (lane == 0) st_flag(&flags[pb.b], make_flag(kFlagIncl, epoch, prefix + padded));
+  }
+  __syncwarp();
+  encode_store<kSlots>(out, out_cap, n, p, pdf, out_size64, out_size32, sink, pb.b, pb.nw, prefix,
+                       pb.x, pb.sout, lane);
+}
+
+// One block as the unit of the single-pass prefix (flags per block): encode,
+// publish the aggregate, look back, store.
 template <bool kSlots, typename TabT>
 __device__ __forceinline__ void encode_block(
     const uint8_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ out, uint64_t out_cap,
@@ -248,14 +282,8 @@ __device__ __forceinline__ void encode_block(
   const uint32_t nw = encode_words(in, n, b, table, stage, bar, parity, sout, p, sink, lane, x);
   const uint32_t padded = (nw + 7) & ~7u;
   if (lane == 0) st_flag(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, padded));
-  uint32_t prefix = 0;
-  if (b > 0) {
-    prefix = lookback_exclusive(flags, b, epoch, sink);
-    if (lane == 0) st_flag(&flags[b], make_flag(kFlagIncl, epoch, prefix + padded));
-  }
-  __syncwarp();
-  encode_store<kSlots>(out, out_cap, n, p, pdf, out_size64, out_size32, sink, b, nw, prefix, x,
-                       sout, lane);
+  encode_finish<kSlots>(out, out_cap, n, out_size64, out_size32, pdf, flags, epoch, p, sink,
+                        EncPending{b, nw, x, sout}, lane);
 }
 
 constexpr int kDecWarps = 8;
@@ -293,22 +321,130 @@ __device__ __forceinline__ bool build_decode_tables(const uint8_t* __restrict__ 
   return true;
 }
 
+// ---- decode ----
+// Words staged in shared memory per warp (4 KiB): every block whose padded
+// word count fits -- all blocks of data that compresses at all -- decodes
+// from shared memory; a block with more words (a block of nearly
+// incompressible bytes) reads its words from global memory instead.
+constexpr uint32_t kDecStageWords = 2048;
+// Decoded bytes leave through a per-warp 512-byte stage, 16 steps at a time,
+// as one 16-byte store per lane.
+constexpr int kDecChunkSteps = 16;
+constexpr uint32_t kDecChunkBytes = kDecChunkSteps * 32;
+
+struct DecWarpSmem {
+  alignas(16) uint16_t words[kDecStageWords];
+  alignas(16) uint8_t out[kDecChunkBytes + 16];  // a chunk at its destination's phase
+};
+
+__device__ __forceinline__ uint32_t ld_shared_u16(uint32_t addr) {
+  uint16_t v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_shared_u32(uint32_t addr) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
+  return v;
+}
+
+// Store one decoded 512-byte chunk from the warp's stage, where it sits at
+// offset ph = g & 15 (the destination's phase), to g: 16-byte stores for the
+// whole 16-byte units and byte stores for a partial first and last unit (the
+// mapped buffer that a MANS decode writes starts at any phase).
+__device__ __forceinline__ void dec_flush_chunk(uint8_t* __restrict__ g, const uint8_t* ostage,
+                                                uint32_t ph, int lane) {
+  if (ph == 0) {
+    reinterpret_cast<uint4*>(g)[lane] = reinterpret_cast<const uint4*>(ostage)[lane];
+    return;
+  }
+  uint8_t* g0 = g - ph;  // 16-byte aligned; stage unit u <-> g0 + 16 u
+  if (lane >= 1) reinterpret_cast<uint4*>(g0)[lane] = reinterpret_cast<const uint4*>(ostage)[lane];
+  if (lane < 16) {
+    if ((uint32_t)lane >= ph) g0[lane] = ostage[lane];                  // unit 0
+    else g0[kDecChunkBytes + lane] = ostage[kDecChunkBytes + lane];      // unit 32
+  }
+}
+
+// The 128 steps of a full block whose words are staged in shared memory, for
+// precision kP. State x per lane; wa: shared byte address one past the next
+// word to read (words are read backwards, the highest reading lane first,
+// GpuANSDecode.h:78-92); lut: shared address of the slot table. Each step:
+// slot -> table entry {pdf:12, slot - cdf:12, symbol:8}; x = pdf * (x >> p) +
+// (slot - cdf); lanes whose state fell below 2^15 read one word each.
+// A corrupt stream can move wa below the warp's words, by at most 128 steps x
+// 32 words = 8 KiB; the slot table (8 KiB) lies below every warp's words in
+// the CTA's shared memory, so such reads stay inside it, and the final
+// position check reports the block. Returns false when the block does not
+// end exactly at its first word in the start state.
+template <int kP>
+__device__ __forceinline__ bool decode_full_smem(uint32_t x, uint32_t wa, uint32_t wa_end,
+                                                 uint32_t lut, uint8_t* __restrict__ dst,
+                                                 uint8_t* ostage, int lane) {
+  constexpr uint32_t kMask = (1u << kP) - 1u;
+  const uint32_t ltmask = lanemask_lt();
+  const uint32_t ph = phase16(dst);  // dst + 512 c has the same phase
+  uint8_t* st = ostage + ph + lane;
+#pragma unroll 1
+  for (int c = kAnsStepsPerBlock / kDecChunkSteps - 1; c >= 0; --c) {
+#pragma unroll
+    for (int i = kDecChunkSteps - 1; i >= 0; --i) {
+      const uint32_t e = ld_shared_u32(lut + ((x & kMask) << 2));
+      st[i * 32] = (uint8_t)e;
+      x = (e >> 20) * (x >> kP) + ((e >> 8) & 0xfffu);
+      const bool rd = x < kAnsStartState;
+      const uint32_t vote = __ballot_sync(0xffffffffu, rd);
+      wa -= 2u * __popc(vote);
+      if (rd) x = (x << 16) | ld_shared_u16(wa + 2u * __popc(vote & ltmask));
+    }
+    __syncwarp();
+    dec_flush_chunk(dst + kDecChunkBytes * c, ostage, ph, lane);
+    __syncwarp();
+  }
+  return wa == wa_end && x == kAnsStartState;
+}
+
+// Any block (partial last block, or words in global memory): the same steps
+// with byte stores and a clamped word index. words: the block's first word
+// (shared or global); ptr: its word count.
+__device__ __forceinline__ bool decode_any(uint32_t x, const uint16_t* words, int ptr, uint32_t bs,
+                                           int p, const uint32_t* lut, uint8_t* __restrict__ dst,
+                                           int lane) {
+  const uint32_t mask = (1u << p) - 1u;
+  const uint32_t gemask = lanemask_ge();
+  const uint32_t rem = bs & 31;
+  int j = (int)((bs + 31) >> 5) - 1;
+  for (; j >= 0; --j) {
+    const bool valid = rem == 0 || j < (int)(bs >> 5) || (uint32_t)lane < rem;
+    if (valid) {
+      const uint32_t e = lut[x & mask];
+      dst[j * 32 + lane] = (uint8_t)e;
+      x = (e >> 20) * (x >> p) + ((e >> 8) & 0xfffu);
+    }
+    const bool rd = valid && x < kAnsStartState;
+    const uint32_t vote = __ballot_sync(0xffffffffu, rd);
+    // a read below the block's first word only happens in a corrupt stream;
+    // it is clamped here and caught by the final position check
+    if (rd) x = x * 65536u + words[max(ptr - __popc(vote & gemask), 0)];
+    ptr -= __popc(vote);
+  }
+  return ptr == 0 && x == kAnsStartState;
+}
+
 // Decode block b of one stream (one warp) into out + 4096 b. in: the stream
 // (header validated by the caller: nb blocks, n bytes, cw words, precision
-// p); lut: the slot table; sin / bar / parity: the warp's word stage.
+// p); lut: the slot table in shared memory (2^11 words, placed below every
+// warp's stage); ws / bar / parity: the warp's stage and its mbarrier.
 __device__ __forceinline__ void decode_block(const uint8_t* __restrict__ in, uint32_t nb,
                                              uint32_t n, uint32_t cw, int p,
                                              uint8_t* __restrict__ out, const uint32_t* lut,
-                                             uint16_t* sin, uint64_t* bar,
-                                             uint32_t& parity, const Sink& sink, uint32_t b,
-                                             int lane) {
+                                             DecWarpSmem* ws, uint64_t* bar, uint32_t& parity,
+                                             const Sink& sink, uint32_t b, int lane) {
   const uint64_t over = ans_overhead(nb);
   const uint32_t* states = reinterpret_cast<const uint32_t*>(in + kAnsHeaderBytes + 2 * kAnsSyms);
   const uint2* bwords = reinterpret_cast<const uint2*>(in + kAnsHeaderBytes + 2 * kAnsSyms + 128ull * nb);
-  const uint8_t* data = in + over;
-  const uint32_t mask = (1u << p) - 1u;
-  const uint32_t gemask = lanemask_ge();
-  uint32_t x = __ldg(states + (uint64_t)b * 32 + lane);
+  const uint16_t* data = reinterpret_cast<const uint16_t*>(in + over);
+  const uint32_t x = __ldg(states + (uint64_t)b * 32 + lane);
   const uint2 bw = __ldg(bwords + b);
   const uint32_t bs = bw.x >> 16, nw = bw.x & 0xffffu, pre = bw.y;
   const uint32_t expect = (b + 1 == nb) ? n - b * kAnsBlock : kAnsBlock;
@@ -317,48 +453,31 @@ __device__ __forceinline__ void decode_block(const uint8_t* __restrict__ in, uin
     if (lane == 0) report(sink, MANS_ERR_CORRUPT, b);
     return;
   }
-  // stage the block's words with one bulk copy (16-byte aligned: over % 16
-  // == 0, pre % 8 == 0); the previous block's reads of the stage are done
-  __syncwarp();
-  if (padded) {
-    if (lane == 0) bulk_load(sin, data + 2ull * pre, 2 * padded, bar);
-    if (!mbar_wait(bar, parity) && lane == 0) report(sink, MANS_ERR_TIMEOUT, b);
-    parity ^= 1u;
-  }
-  uint8_t* dst = out + (uint64_t)b * kAnsBlock + lane;
-  int ptr = (int)nw;
-  bool bad;
-  const uint32_t rem = bs & 31;
-  int j = (int)((bs + 31) >> 5) - 1;
-  if (rem) {
-    const bool valid = (uint32_t)lane < rem;
-    if (valid) {
-      const uint32_t s0 = x & mask;
-      const uint32_t e = lut[s0];
-      dst[j * 32] = (uint8_t)e;
-      x = (e >> 20) * (x >> p) + ((e >> 8) & 0xfffu);
+  uint8_t* dst = out + (uint64_t)b * kAnsBlock;
+  bool ok;
+  if (padded <= kDecStageWords) {
+    // stage the block's words with one bulk copy (16-byte aligned: over % 16
+    // == 0, pre % 8 == 0); the previous block's reads of the stage are done
+    __syncwarp();
+    if (padded) {
+      if (lane == 0) bulk_load(ws->words, data + pre, 2 * padded, bar);
+      if (!mbar_wait(bar, parity) && lane == 0) report(sink, MANS_ERR_TIMEOUT, b);
+      parity ^= 1u;
     }
-    const bool rd = valid && x < kAnsStartState;
-    const uint32_t vote = __ballot_sync(0xffffffffu, rd);
-    if (rd) x = x * 65536u + sin[max(ptr - __popc(vote & gemask), 0)];
-    ptr -= __popc(vote);
-    --j;
+    if (bs == kAnsBlock) {
+      const uint32_t w0 = smem_addr(ws->words), l0 = smem_addr(lut);
+      switch (p) {
+        case 9: ok = decode_full_smem<9>(x, w0 + 2 * nw, w0, l0, dst, ws->out, lane); break;
+        case 10: ok = decode_full_smem<10>(x, w0 + 2 * nw, w0, l0, dst, ws->out, lane); break;
+        default: ok = decode_full_smem<11>(x, w0 + 2 * nw, w0, l0, dst, ws->out, lane); break;
+      }
+    } else {
+      ok = decode_any(x, ws->words, (int)nw, bs, p, lut, dst, lane);
+    }
+  } else {
+    ok = decode_any(x, data + pre, (int)nw, bs, p, lut, dst, lane);
   }
-#pragma unroll 4
-  for (; j >= 0; --j) {
-    const uint32_t s0 = x & mask;
-    const uint32_t e = lut[s0];
-    dst[j * 32] = (uint8_t)e;
-    x = (e >> 20) * (x >> p) + ((e >> 8) & 0xfffu);
-    const bool rd = x < kAnsStartState;
-    const uint32_t vote = __ballot_sync(0xffffffffu, rd);
-    // A read below the block's first word only happens in a corrupt
-    // stream; it is clamped here and caught by the final ptr check.
-    if (rd) x = x * 65536u + sin[max(ptr - __popc(vote & gemask), 0)];
-    ptr -= __popc(vote);
-  }
-  bad = ptr != 0 || x != kAnsStartState;
-  if (__any_sync(0xffffffffu, bad) && lane == 0) report(sink, MANS_ERR_CORRUPT, b);
+  if (__any_sync(0xffffffffu, !ok) && lane == 0) report(sink, MANS_ERR_CORRUPT, b);
 }
 
 }  // namespace mans

@@ -522,8 +522,8 @@ __global__ __launch_bounds__(32) void batch_plan_decode_kernel(const BatchItem* 
 // buffer stay in shared memory until the CTA moves to another buffer.
 // ------------------------------------------------------------------------
 struct BatchDecSmem {
-  uint32_t lut[1 << kMaxProbBits];
-  alignas(16) uint16_t in[kBWarps][kEncOutWords];
+  uint32_t lut[1 << kMaxProbBits];  // below every warp's stage (see decode_full_smem)
+  DecWarpSmem warp[kBWarps];
   uint64_t bar[kBWarps];
 };
 
@@ -563,7 +563,7 @@ __global__ __launch_bounds__(kBThreads) void batch_decode_kernel(const BatchItem
     const uint32_t blk = (c - st->unit_base) * kChunkBlocks + warp;
     if (blk < st->nb) {
       uint8_t* dst = b.dtype == MANS_U8 ? b.out : b.m;
-      decode_block(b.in, st->nb, st->n_hdr, st->cw, (int)p, dst, sm.lut, sm.in[warp], bar,
+      decode_block(b.in, st->nb, st->n_hdr, st->cw, (int)p, dst, sm.lut, &sm.warp[warp], bar,
                    parity, item_sink(ctrl, st), blk, lane);
     }
   }
