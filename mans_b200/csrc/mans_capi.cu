@@ -123,9 +123,13 @@ uint64_t ans_stream_bound(uint64_t n) { return ans_bound(n); }
 namespace {
 
 // Copy the mapped bytes (size in ctrl) out of the workspace, with a capacity
-// check; thread 0 stores the size.
+// check; thread 0 stores the size. It ends a map-only call, so it also
+// advances the look-back epoch (in a compress the encoder does), which the
+// mapping kernels before it have read: the next call's flags then never
+// match this call's.
 __global__ void export_merged_kernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
                                      uint64_t cap, Ctrl* ctrl, unsigned long long* out_size) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->epoch = (ctrl->epoch + 1) & 0x3fffffffu;
   if (*((volatile uint32_t*)&ctrl->status) != 0) return;
   const uint64_t n = __ldcg(&ctrl->merged_size);
   if (n > cap) {

@@ -51,6 +51,23 @@ def test_u32_native_mapping_matches_oracle(ws, oracle):
         np.testing.assert_array_equal(to_host(back, np.uint32), x)
 
 
+@pytest.mark.parametrize("dtype", ["u16", "u32"])
+def test_map_only_calls_in_a_row_with_new_data(ws, oracle, dtype):
+    """Consecutive map-only calls (and a compress after them) on one workspace
+    with different data of the same size: the look-back flags of one call
+    must never be read as valid by the next, whatever the data."""
+    n = 300_000
+    gens = (W.gradient_u16, W.volume_u16, W.laplace_u16) if dtype == "u16" else \
+        (W.quant_u32, W.detector_u32, W.quant_u32)
+    for i, gen in enumerate(gens):
+        x = gen(n, 900 + i)
+        dx = to_dev(x)
+        ref = oracle.adm_u16_map(x) if dtype == "u16" else oracle.adm_u32_map(x)
+        np.testing.assert_array_equal(to_host(mb.adm_map(dx, ws=ws)), ref, err_msg=f"call {i}")
+    y = gens[0](n, 990)
+    np.testing.assert_array_equal(to_host(mb.compress(to_dev(y), 10, ws=ws)), oracle.compress(y, 10))
+
+
 def test_layout_header_corruption_is_reported(ws, oracle):
     import torch
     n = 70001
