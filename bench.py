@@ -75,6 +75,11 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="override the element count (profiling runs)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="default workload: skip the mixed_c3 / serve_c5 / reference_gpu sub-records")
+    ap.add_argument("--sub-steps", type=int, default=3, help="mixed_c3 sub-record: timed steps")
+    ap.add_argument("--sub-requests", type=int, default=20_000,
+                    help="serve_c5 sub-record: requests of the Poisson trace")
     ap.add_argument("--traffic-json", default=os.path.join(ROOT, "profiles", "dram_traffic.json"),
                     help="ncu-measured DRAM bytes per launch of each kernel (roofline.traffic)")
     ap.add_argument("--no-check-oracle", action="store_true",
@@ -592,7 +597,7 @@ def run_mans(args):
                         "against the oracle's group- and block-parallel restatement "
                         "(oracle/mans_oracle.c), after the timed region",
                 "seconds": round(time.time() - t0, 1)}
-        print(json.dumps(result), flush=True)
+    return result
 
 
 # ---------------------------------------------------------------- mixed batch
@@ -800,7 +805,7 @@ def run_mixed(args):
     except Exception:
         avail = 0
     need = total + out_total + total
-    if avail > 2 * need:
+    if avail > 2 * need and not getattr(args, "no_e2e", False):
         del gbc, gbd
         batch.close()
         n_chunks = 8
@@ -917,10 +922,9 @@ def run_mixed(args):
     if batch is not None:
         batch.close()
     ws.close()
-    if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = mixed_cpu_sample(reps=3, warm=1)
-        print(json.dumps(result), flush=True)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = mixed_cpu_sample(reps=3, warm=1)
+    return result
 
 
 # ---------------------------------------------------------------- serving
@@ -1092,7 +1096,8 @@ def run_serve(args):
         "gpu_launches": None,
     }
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 def check_oracle(args, x, s) -> bool:
@@ -1105,16 +1110,178 @@ def check_oracle(args, x, s) -> bool:
     return bool(got.size == want.size and np.array_equal(got, want))
 
 
+def _parse_floats(text: str, keys: dict) -> dict:
+    out = {}
+    for name, label in keys.items():
+        for line in text.splitlines():
+            if label in line:
+                try:
+                    out[name] = float(line.split(label, 1)[1].strip().split()[0])
+                except (ValueError, IndexError):
+                    pass
+    return out
+
+
+def _ours_per_stage(x, reps: int = 10) -> dict:
+    """Per-kernel milliseconds of this library on device tensor x (events
+    the library records around each launch), after warm-up."""
+    import torch
+
+    import mans_b200 as mb
+    n = x.numel()
+    ws = mb.Workspace(n * x.element_size())
+    cap = mb.max_compressed_size(mb.dtype_code(x), n)
+    out = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    size = torch.zeros(1, dtype=torch.int64, device="cuda")
+    back = torch.empty_like(x)
+    for _ in range(3):
+        mb.compress_into(ws, x, out, size, 10)
+        mb.decompress_into(ws, out, cap, back)
+    ws.check(None, "warm-up")
+    ws.set_timing(True)
+    for _ in range(reps):
+        mb.compress_into(ws, x, out, size, 10)
+        mb.decompress_into(ws, out, cap, back)
+    kt = ws.kernel_times()
+    ws.set_timing(False)
+    ws.check(None, "timed")
+    ok = bool(torch.equal(back.view(torch.uint8), x.view(torch.uint8)))
+    ws.close()
+    c, d = max(1, kt["compress_calls"]), max(1, kt["decompress_calls"])
+    r = {"map_ms": kt["map"] / c, "encode_ms": kt["encode"] / c, "decode_ms": kt["decode"] / d,
+         "unmap_ms": kt["unmap"] / d, "round_trip_ok": ok}
+    return {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
+
+
+def reference_gpu(args) -> dict:
+    """The reference's own GPU path, built from its sources under oracle/_ref
+    (oracle/Makefile), timed on this GPU on the same inputs as this library:
+    the V15 uint16 mapper (mapping/nv/mappingV15_fused_uint16.cu, its own
+    CUDA-event timing, :856-869 and :971-985) and the V9 uint32 mapper
+    (mapping/nv/mappingV9_fuse.cu:841-919) each followed by the include/ans
+    codec (ansEncode / ansDecode, timed by oracle/ref_ans_driver in its
+    "time" mode: CUDA events and a host clock per call as
+    examples/compress.cu:45-63). Inputs the reference handles: config 1
+    (4,194,304 uint16) and a 2^27-element slice of the uint32 detector
+    frames (the reference's uint32 mapper sizes its scratch with an int and
+    fails at 2^28 elements, mappingV9_fuse.cu:803). Lazy module loading is
+    off (CUDA_MODULE_LOADING=EAGER) so that no kernel's first launch pays for
+    loading code."""
+    import subprocess
+    import tempfile
+
+    import torch
+
+    from mans_b200 import workloads as W
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    bins = {k: os.path.join(ref, k) for k in ("mappingV15", "mappingV9", "ref_ans_driver")}
+    missing = [k for k, v in bins.items() if not os.path.exists(v)]
+    if missing:
+        return {"unavailable": f"reference binaries not built: {', '.join(missing)}"}
+    env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+    res = {"what": "per-stage milliseconds of the reference's GPU code and of this library on "
+                   "the same inputs, same GPU, same run"}
+
+    def run(cmd):
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"{os.path.basename(cmd[0])} rc={r.returncode}: {r.stderr[-300:]}")
+        return r.stdout
+
+    with tempfile.TemporaryDirectory() as td:
+        cases = [("laplace_u16_c1", W.laplace_u16(W.C1_N, 1), "mappingV15"),
+                 ("detector_u32_2p27", W.detector_u32(1 << 27, 2), "mappingV9")]
+        for name, x, mapper in cases:
+            fi, fm = os.path.join(td, name + ".bin"), os.path.join(td, name + ".adm")
+            x.tofile(fi)
+            rec = {"elements": int(x.size), "bytes": int(x.nbytes)}
+            if mapper == "mappingV15":
+                txt = run([bins[mapper], fi, fm])
+                rec["reference"] = _parse_floats(txt, {
+                    "map_ms": "Total Cmp Time:", "map_adm_kernel_ms": "ADM cost",
+                    "map_prefix_sum_ms": "Prefix-sum cost", "map_concat_ms": "Concat cost",
+                    "unmap_ms": "Total cost"})
+            else:
+                txt = run([bins[mapper], fi, fm, "uint32"])
+                rec["reference"] = _parse_floats(txt, {"map_ms": "Compression cost",
+                                                       "unmap_ms": "Decompression cost"})
+            rec["reference"]["mapped_bytes"] = os.path.getsize(fm)
+            txt = run([bins["ref_ans_driver"], "time", "10", fm, "5"])
+            line = next((l for l in txt.splitlines() if l.startswith("REFTIME")), "")
+            kv = dict(t.split("=", 1) for t in line.split()[1:] if "=" in t)
+            rec["reference"].update({
+                "encode_ms": float(kv.get("encode_event_ms", "nan")),
+                "encode_wall_ms": float(kv.get("encode_wall_ms", "nan")),
+                "decode_ms": float(kv.get("decode_event_ms", "nan")),
+                "decode_wall_ms": float(kv.get("decode_wall_ms", "nan")),
+                "rans_round_trip_ok": kv.get("roundtrip") == "ok"})
+            rec["reference"]["pipeline_ms"] = round(sum(
+                rec["reference"].get(k, 0.0) for k in ("map_ms", "encode_ms", "decode_ms", "unmap_ms")), 4)
+            d = torch.from_numpy(x.view(np.uint8).copy()).cuda().view(
+                torch.uint16 if x.dtype == np.uint16 else torch.uint32)
+            rec["mans"] = _ours_per_stage(d)
+            rec["mans"]["pipeline_ms"] = round(sum(
+                rec["mans"][k] for k in ("map_ms", "encode_ms", "decode_ms", "unmap_ms")), 4)
+            rec["speedup"] = round(rec["reference"]["pipeline_ms"] / rec["mans"]["pipeline_ms"], 2) \
+                if rec["mans"]["pipeline_ms"] else None
+            res[name] = rec
+            del d
+    return res
+
+
+def sub_records(args) -> dict:
+    """The batched (config 3) and served (config 5) forms and the reference's
+    own GPU path, measured after the single-buffer headline in the same run
+    (one GPU): the metric's "batched vs plain" and "p50/p99 latency" parts."""
+    import copy
+
+    import torch
+    out = {}
+    sub = copy.copy(args)
+    torch.cuda.empty_cache()  # the headline's buffers, cached by torch
+    sub.no_cpu_baseline = True
+    t0 = time.time()
+    try:
+        sub.items, sub.steps, sub.warmup, sub.no_e2e = 0, args.sub_steps, 3, True
+        out["mixed_c3"] = run_mixed(sub)
+        out["mixed_c3"]["seconds"] = round(time.time() - t0, 1)
+    except Exception as e:  # reported, never hidden
+        out["mixed_c3"] = {"error": f"{type(e).__name__}: {e}"}
+    torch.cuda.empty_cache()  # the serving loop reserves its whole HBM budget up front
+    t0 = time.time()
+    try:
+        sub.requests, sub.steps = args.sub_requests, 1
+        out["serve_c5"] = run_serve(sub)
+        out["serve_c5"]["seconds"] = round(time.time() - t0, 1)
+    except Exception as e:
+        out["serve_c5"] = {"error": f"{type(e).__name__}: {e}"}
+    torch.cuda.empty_cache()
+    t0 = time.time()
+    try:
+        out["reference_gpu"] = reference_gpu(args)
+        out["reference_gpu"]["seconds"] = round(time.time() - t0, 1)
+    except Exception as e:
+        out["reference_gpu"] = {"error": f"{type(e).__name__}: {e}"}
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "mixed_c3":
-        run_mixed(args)
+        return
+    if args.workload == "mixed_c3":
+        line = run_mixed(args)
     elif args.workload == "serve_c5":
-        run_serve(args)
+        line = run_serve(args)
     else:
-        run_mans(args)
+        line = run_mans(args)
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        if line is not None and world == 1 and args.workload == "detector_u32" and not args.n \
+                and not args.no_sub:
+            line.update(sub_records(args))
+    if line is not None:
+        print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

@@ -76,16 +76,24 @@ __device__ __forceinline__ uint32_t enc_threshold(const EncEntry4& e) {
 // One interleaved step: renormalise (emit 16 bits, lanes in ascending order
 // into the compacted word buffer), then code the symbol.
 // kGuard: drop words past the buffer (see encode_words).
-template <int kP, bool kGuard, typename TabT>
+template <int kP, bool kGuard, bool kShared, typename TabT>
 __device__ __forceinline__ void enc_step(bool valid, uint32_t& x, uint32_t sym,
                                          const TabT* __restrict__ tab, uint16_t* __restrict__ out,
                                          uint32_t& nw, uint32_t ltmask) {
   const TabT e = tab[sym];
   const bool wr = valid && x >= enc_threshold<kP>(e);
   const uint32_t vote = __ballot_sync(0xffffffffu, wr);
-  if (wr) {
-    const uint32_t idx = nw + __popc(vote & ltmask);
-    if (!kGuard || idx < kEncOutWords) out[idx] = (uint16_t)(x & 0xffffu);
+  const uint32_t idx = nw + __popc(vote & ltmask);
+  const bool st = wr && (!kGuard || idx < kEncOutWords);
+  if constexpr (kShared) {
+    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %2, 0;\n @q st.shared.u16 [%0], %1;\n}\n"
+                 ::"r"((uint32_t)__cvta_generic_to_shared(out + idx)), "h"((uint16_t)x),
+                 "r"((uint32_t)st)
+                 : "memory");
+  } else {
+    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %2, 0;\n @q st.global.u16 [%0], %1;\n}\n"
+                 ::"l"(out + idx), "h"((uint16_t)x), "r"((uint32_t)st)
+                 : "memory");
   }
   nw += __popc(vote);
   const uint32_t xr = wr ? (x >> 16) : x;
@@ -97,9 +105,9 @@ __device__ __forceinline__ void discard_l2_line(const void* p) {
 }
 
 // The coding of one staged block (syms: the lane's first symbol in the stage,
-// bs bytes) at precision kP, symbols read eight steps ahead. Returns the word
-// count; x receives the lane's final state.
-template <int kP, typename TabT>
+// bs bytes) at precision kP. kShared: sout is in shared memory (else a
+// global slot). Returns the word count; x receives the lane's final state.
+template <int kP, bool kShared, typename TabT>
 __device__ __forceinline__ uint32_t encode_staged(const uint8_t* syms, uint32_t bs,
                                                   const TabT* table, uint16_t* sout, int lane,
                                                   uint32_t& x) {
@@ -109,47 +117,39 @@ __device__ __forceinline__ uint32_t encode_staged(const uint8_t* syms, uint32_t 
   const uint32_t full = bs >> 5;
   uint32_t j = 0;
   // Each step adds at most 32 words, and nw is the same in every lane: while
-  // nw <= kRoom the next eight steps fit in the buffer without a check.
+  // nw <= kRoom the next eight steps fit in the buffer without a check. The
+  // eight symbol loads of a round do not depend on the state, so they issue
+  // ahead of the round's coding chain.
   constexpr uint32_t kRoom = kEncOutWords - 8 * 32;
-  if (full >= 8) {
-    uint32_t cur[8];
+  for (; j + 8 <= full && nw <= kRoom; j += 8) {
 #pragma unroll
-    for (int u = 0; u < 8; ++u) cur[u] = syms[u * 32];
-    for (; j + 16 <= full && nw <= kRoom; j += 8) {
-      uint32_t nx[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) nx[u] = syms[(j + 8 + u) * 32];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) enc_step<kP, false>(true, x, cur[u], table, sout, nw, ltmask);
-#pragma unroll
-      for (int u = 0; u < 8; ++u) cur[u] = nx[u];
-    }
-    if (nw <= kRoom) {
-#pragma unroll
-      for (int u = 0; u < 8; ++u) enc_step<kP, false>(true, x, cur[u], table, sout, nw, ltmask);
-      j += 8;
-    }
+    for (int u = 0; u < 8; ++u)
+      enc_step<kP, false, kShared>(true, x, syms[(j + u) * 32], table, sout, nw, ltmask);
   }
   const bool tail_valid = (uint32_t)lane < (bs & 31);
-  if (nw <= kRoom && full - j <= 7) {  // at most eight more steps
-    for (; j < full; ++j) enc_step<kP, false>(true, x, syms[j * 32], table, sout, nw, ltmask);
+  if (nw <= kRoom) {  // at most seven more steps and the partial one
+    for (; j < full; ++j)
+      enc_step<kP, false, kShared>(true, x, syms[j * 32], table, sout, nw, ltmask);
     if (bs & 31)
-      enc_step<kP, false>(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw, ltmask);
+      enc_step<kP, false, kShared>(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw,
+                                   ltmask);
   } else {
-    for (; j < full; ++j) enc_step<kP, true>(true, x, syms[j * 32], table, sout, nw, ltmask);
+    for (; j < full; ++j)
+      enc_step<kP, true, kShared>(true, x, syms[j * 32], table, sout, nw, ltmask);
     if (bs & 31)
-      enc_step<kP, true>(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw, ltmask);
+      enc_step<kP, true, kShared>(tail_valid, x, tail_valid ? syms[j * 32] : 0u, table, sout, nw,
+                                  ltmask);
   }
   return nw;
 }
 
 // Encode block b of one buffer (one warp) into the warp's word buffer sout
-// (with kSlots a per-warp slot in global memory, which stays in L2, else
-// shared memory): one bulk copy of the block into the warp's stage, then the
+// (kSharedOut: in shared memory, else a per-warp slot in global memory,
+// which stays in L2): one bulk copy of the block into the warp's stage, then the
 // interleaved coding; the word count is padded to a 16-byte multiple with
 // zeros (GpuANSEncode.h:275). Returns the number of words; x receives the
 // lane's final state.
-template <typename TabT>
+template <bool kSharedOut, typename TabT>
 __device__ __forceinline__ uint32_t encode_words(const uint8_t* __restrict__ in, uint64_t n,
                                                  uint32_t b, const TabT* table, uint8_t* stage,
                                                  uint64_t* bar, uint32_t& parity, uint16_t* sout,
@@ -169,9 +169,9 @@ __device__ __forceinline__ uint32_t encode_words(const uint8_t* __restrict__ in,
   const uint8_t* syms = stage + phase16(in + start) + lane;
   uint32_t nw;
   switch (p) {
-    case 9: nw = encode_staged<9>(syms, bs, table, sout, lane, x); break;
-    case 10: nw = encode_staged<10>(syms, bs, table, sout, lane, x); break;
-    default: nw = encode_staged<11>(syms, bs, table, sout, lane, x); break;
+    case 9: nw = encode_staged<9, kSharedOut>(syms, bs, table, sout, lane, x); break;
+    case 10: nw = encode_staged<10, kSharedOut>(syms, bs, table, sout, lane, x); break;
+    default: nw = encode_staged<11, kSharedOut>(syms, bs, table, sout, lane, x); break;
   }
   // A table that fits the block's bytes keeps each lane within its bound of
   // words (kAnsMaxBlockWords / 32); only a table built from other bytes (two
@@ -279,7 +279,8 @@ __device__ __forceinline__ void encode_block(
     unsigned long long* flags, uint32_t epoch, int p, const Sink& sink, const TabT* table,
     uint8_t* stage, uint64_t* bar, uint32_t& parity, uint16_t* sout, uint32_t b, int lane) {
   uint32_t x;
-  const uint32_t nw = encode_words(in, n, b, table, stage, bar, parity, sout, p, sink, lane, x);
+  const uint32_t nw =
+      encode_words<!kSlots>(in, n, b, table, stage, bar, parity, sout, p, sink, lane, x);
   const uint32_t padded = (nw + 7) & ~7u;
   if (lane == 0) st_flag(&flags[b], make_flag(b == 0 ? kFlagIncl : kFlagAgg, epoch, padded));
   encode_finish<kSlots>(out, out_cap, n, out_size64, out_size32, pdf, flags, epoch, p, sink,
