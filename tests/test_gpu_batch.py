@@ -103,7 +103,7 @@ def test_batch_edge_sizes_match_single_and_oracle(ws, batch, oracle):
         np.testing.assert_array_equal(y, x, err_msg=f"item {i}")
 
 
-def test_batch_mixed_sizes_match_single(ws, batch):
+def test_batch_mixed_sizes_match_single(ws, batch, oracle):
     sizes_b = W.mixed_sizes(96, seed=11, lo=4 << 10, hi=2 << 20)
     kinds = ("u16", "u32", "u8")
     xs = []
@@ -114,6 +114,8 @@ def test_batch_mixed_sizes_match_single(ws, batch):
     first, st, streams = run_compress(batch, xs, ps)
     assert first == 0 and not any(st)
     for i, (x, s) in enumerate(zip(xs, streams)):
+        ref = oracle.compress_par(x, 10) if x.dtype != np.uint8 else oracle.ans_encode(x, 10)
+        np.testing.assert_array_equal(s, ref, err_msg=f"item {i} against the oracle")
         np.testing.assert_array_equal(s, single_stream(ws, x, 10), err_msg=f"item {i}")
     first, st, back = run_decompress(batch, streams, xs)
     assert first == 0 and not any(st)

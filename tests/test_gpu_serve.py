@@ -166,3 +166,38 @@ def test_server_caller_owned_outputs(ws):
         assert srv.stats()["arena_used"] == 0
     finally:
         srv.close()
+
+
+def test_server_admits_requests_while_a_batch_runs(ws, oracle):
+    """Continuous batching: with one lane per direction, a 1 GiB compress
+    request occupies the compress lane for milliseconds; 16 small requests
+    submitted meanwhile (while it is in flight) are admitted, wait for the
+    lane, and then run together in one batch of more than one item. Every
+    small result equals the oracle's stream of that request alone."""
+    import torch
+    big = W.gen_device("volume_u16", 1 << 29, 31)
+    smalls = [W.gradient_u16(65_536 + 512 * i, 400 + i) for i in range(16)]
+    ds = [to_dev(x) for x in smalls]
+    srv = serve.Server(8 << 30, max_batch_bytes=(1 << 30) + (64 << 20), max_batch_items=64, lanes=1)
+    try:
+        torch.cuda.synchronize()
+        t_big = srv.submit(serve.COMPRESS, 2, big.numel(), big.data_ptr(), precision=10, tag=999)
+        import time
+        t0 = time.time()
+        while srv.stats()["in_flight"] == 0 and srv.stats()["completed"] == 0:
+            assert time.time() - t0 < 10, "the large request was never dispatched"
+        in_flight_before = srv.stats()["in_flight"]
+        tick = [srv.submit(serve.COMPRESS, 2, x.size, d.data_ptr(), precision=10, tag=i)
+                for i, (x, d) in enumerate(zip(smalls, ds))]
+        still_running = srv.stats()["completed"] == 0
+        done = drain(srv, len(tick) + 1)
+        assert in_flight_before >= 1 and still_running, "the large request finished too early"
+        assert done[t_big][0].status == 0 and done[t_big][0].batch_items == 1
+        items = [done[t][0].batch_items for t in tick]
+        assert max(items) > 1, items
+        for i, t in enumerate(tick):
+            c, data = done[t]
+            assert c.status == 0
+            np.testing.assert_array_equal(data, oracle.compress(smalls[i], 10), err_msg=f"request {i}")
+    finally:
+        srv.close()
