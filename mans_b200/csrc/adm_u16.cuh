@@ -99,6 +99,26 @@ struct Map16Lane {
   int cnt;        // valid elements of the lane
 };
 
+// Codes and unary stream of a lane's elements (kFull: all 16 valid, no
+// per-element branch): code bytes packed into codes, each counted in hist;
+// the stream's first 64 bits in acc, its length in pos.
+template <bool kFull>
+__device__ __forceinline__ void map16_elems(const uint32_t (&w)[8], uint32_t c, int cnt,
+                                            uint32_t* hist, uint32_t (&codes)[4], uint64_t& acc,
+                                            uint32_t& pos) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    if (kFull || i < cnt) {
+      uint32_t k, code;
+      adm_elem_u16(elem16(w, i), c, k, code);
+      codes[i >> 2] |= code << ((i & 3) * 8);
+      atomicAdd(&hist[code], 1u);
+      if (pos < 64) acc |= 0x8000000000000000ull >> pos;
+      pos += k;
+    }
+  }
+}
+
 // First half of mapping group `grp` (one warp): everything that does not
 // depend on the group's offset -- center, codes (stored), the lane bit
 // streams' first 64 bits, the group length and the histogram of the codes
@@ -128,17 +148,8 @@ __device__ __forceinline__ void map16_front(const uint16_t* __restrict__ in, uin
   uint32_t codes[4] = {0, 0, 0, 0};
   uint64_t acc = 0;
   uint32_t pos = 0;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    if (i < a.cnt) {
-      uint32_t k, code;
-      adm_elem_u16(elem16(w, i), a.c, k, code);
-      codes[i >> 2] |= code << ((i & 3) * 8);
-      atomicAdd(&hist[code], 1u);
-      if (pos < 64) acc |= 0x8000000000000000ull >> pos;
-      pos += k;
-    }
-  }
+  if (a.cnt == 16) map16_elems<true>(w, a.c, 16, hist, codes, acc, pos);
+  else map16_elems<false>(w, a.c, a.cnt, hist, codes, acc, pos);
   a.L = __reduce_max_sync(0xffffffffu, (pos + 7) >> 3);
   a.pos = pos;
 
@@ -294,6 +305,34 @@ __device__ __forceinline__ uint32_t rd_u32_2aligned(const uint8_t* p) {
   return (uint32_t)q[0] | ((uint32_t)q[1] << 16);
 }
 
+// The signal counts of a lane's unary stream held left-aligned in acc (L <= 8
+// bytes): per element, the zeros after its leading 1. Returns true when the
+// stream is malformed. kFull: all 16 elements are valid (no per-element
+// branch).
+template <bool kFull>
+__device__ __forceinline__ bool unary_signals(uint64_t acc, int L, int cnt, uint32_t (&sig)[16]) {
+  // win: the stream from the current element's leading 1, left-aligned;
+  // left: its bits that are still in the lane's record
+  uint64_t win = acc;
+  int left = 8 * L;
+  bool bad = false;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    sig[i] = 0;
+    if (kFull || i < cnt) {
+      bad |= left <= 0 || !(win >> 63);
+      const uint64_t rest = win << 1;
+      int z = rest ? __clzll(rest) : 64;
+      const int lim = left > 1 ? left - 1 : 0;
+      z = z < lim ? z : lim;
+      sig[i] = (uint32_t)z;
+      win = z < 63 ? rest << z : 0ull;  // advance by z + 1 bits
+      left -= z + 1;
+    }
+  }
+  return bad;
+}
+
 // Restore group `grp` of one buffer (one warp). tot: bit bytes / 32
 // (validated by the caller). V12 layout: v12_excl holds the exclusive prefix
 // of its u16 lengths (computed by the caller).
@@ -346,24 +385,8 @@ __device__ __forceinline__ void unmap16_group(const uint8_t* __restrict__ M, uin
   if (L <= 8) {
     uint64_t acc = 0;
     for (uint32_t b = 0; b < L; ++b) acc |= (uint64_t)src[b] << (56 - 8 * b);
-    // win: the stream from the current element's leading 1, left-aligned;
-    // left: its bits that are still in the lane's record
-    uint64_t win = acc;
-    int left = 8 * (int)L;
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      sig[i] = 0;
-      if (i < cnt) {
-        if (left <= 0 || !(win >> 63)) bad = true;
-        const uint64_t rest = win << 1;
-        int z = rest ? __clzll(rest) : 64;
-        const int lim = left > 1 ? left - 1 : 0;
-        z = z < lim ? z : lim;
-        sig[i] = (uint32_t)z;
-        win = z < 63 ? rest << z : 0ull;  // advance by z + 1 bits
-        left -= z + 1;
-      }
-    }
+    if (cnt == 16) bad = unary_signals<true>(acc, (int)L, 16, sig);
+    else bad = unary_signals<false>(acc, (int)L, cnt, sig);
   } else {
     // Long lanes: scan byte by byte like the reference.
     int idx = -1;

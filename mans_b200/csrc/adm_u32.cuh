@@ -73,6 +73,53 @@ __device__ __forceinline__ void load_lane_u32(const uint32_t* __restrict__ in, u
   }
 }
 
+// Stage a lane's record at phase 0 as whole 8-byte words: bytes are
+// appended to a 16-byte accumulator (lo, hi) and each completed word is
+// stored once; the last word is padded with 255. Record starts are
+// multiples of 8, so every store is an aligned 8-byte store. kFull: all 16
+// elements are valid (no per-element branch on the byte count).
+template <bool kFull>
+__device__ __forceinline__ void map32_stage(const uint32_t* __restrict__ in, uint64_t ls,
+                                            const uint32_t (&nbp)[2], const uint32_t (&codes)[4],
+                                            uint32_t escm, uint32_t* hist, uint8_t* rec) {
+  uint64_t lo = 0, hi = 0;
+  uint32_t fill = 0, wpos = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const uint32_t nb = (nbp[i >> 3] >> ((i & 7) * 4)) & 0xfu;
+    if (kFull || nb != 0) {
+      if ((escm >> i) & 1u) {
+        const uint32_t x = __ldg(in + ls + i);  // re-read: keeps v[] out of the live range
+        // 254 then the value big-endian
+        const uint64_t e = 254ull | ((uint64_t)__byte_perm(x, 0, 0x0123) << 8);
+        lo |= e << (8 * fill);
+        hi |= fill ? e >> (64 - 8 * fill) : 0ull;
+        atomicAdd(&hist[254], 1u);
+        atomicAdd(&hist[x >> 24], 1u);
+        atomicAdd(&hist[(x >> 16) & 0xff], 1u);
+        atomicAdd(&hist[(x >> 8) & 0xff], 1u);
+        atomicAdd(&hist[x & 0xff], 1u);
+      } else {
+        // nb - 1 zero bytes, then the code byte
+        const uint32_t code = (codes[i >> 2] >> ((i & 3) * 8)) & 0xffu;
+        const uint32_t at = fill + nb - 1;  // < 15
+        if (at < 8) lo |= (uint64_t)code << (8 * at);
+        else hi |= (uint64_t)code << (8 * (at - 8));
+        atomicAdd(&hist[code], 1u);
+      }
+      fill += nb;
+      if (fill >= 8) {
+        *reinterpret_cast<uint64_t*>(rec + wpos) = lo;
+        wpos += 8;
+        lo = hi;
+        hi = 0;
+        fill -= 8;
+      }
+    }
+  }
+  if (fill) *reinterpret_cast<uint64_t*>(rec + wpos) = lo | (~0ull << (8 * fill));
+}
+
 // Map group `grp` of one buffer (one warp). flags: the buffer's per-group
 // look-back flags; msize_out: written by the buffer's last group; hist: the
 // warp's shared histogram; stage: the warp's kGroupRecMax + 16 byte stage.
@@ -127,49 +174,8 @@ __device__ __forceinline__ void map32_group(const uint32_t* __restrict__ in, uin
   // publish the group's aggregate now; the prefix is read after staging
   if (lane == 0) st_flag(&flags[grp], make_flag(grp == 0 ? kFlagIncl : kFlagAgg, epoch, gtot));
 
-  // Stage the lane's record at phase 0 as whole 8-byte words: bytes are
-  // appended to a 16-byte accumulator (lo, hi) and each completed word is
-  // stored once; the last word is padded with 255. Record starts are
-  // multiples of 8, so every store is an aligned 8-byte store.
-  {
-    uint8_t* rec = stage + loff;
-    uint64_t lo = 0, hi = 0;
-    uint32_t fill = 0, wpos = 0;
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const uint32_t nb = (nbp[i >> 3] >> ((i & 7) * 4)) & 0xfu;
-      if (nb != 0) {
-        if ((escm >> i) & 1u) {
-          const uint32_t x = __ldg(in + ls + i);  // re-read: keeps v[] out of the live range
-          // 254 then the value big-endian
-          const uint64_t e = 254ull | ((uint64_t)__byte_perm(x, 0, 0x0123) << 8);
-          lo |= e << (8 * fill);
-          hi |= fill ? e >> (64 - 8 * fill) : 0ull;
-          atomicAdd(&hist[254], 1u);
-          atomicAdd(&hist[x >> 24], 1u);
-          atomicAdd(&hist[(x >> 16) & 0xff], 1u);
-          atomicAdd(&hist[(x >> 8) & 0xff], 1u);
-          atomicAdd(&hist[x & 0xff], 1u);
-        } else {
-          // nb - 1 zero bytes, then the code byte
-          const uint32_t code = (codes[i >> 2] >> ((i & 3) * 8)) & 0xffu;
-          const uint32_t at = fill + nb - 1;  // < 15
-          if (at < 8) lo |= (uint64_t)code << (8 * at);
-          else hi |= (uint64_t)code << (8 * (at - 8));
-          atomicAdd(&hist[code], 1u);
-        }
-        fill += nb;
-        if (fill >= 8) {
-          *reinterpret_cast<uint64_t*>(rec + wpos) = lo;
-          wpos += 8;
-          lo = hi;
-          hi = 0;
-          fill -= 8;
-        }
-      }
-    }
-    if (fill) *reinterpret_cast<uint64_t*>(rec + wpos) = lo | (~0ull << (8 * fill));
-  }
+  if (cnt == 16) map32_stage<true>(in, ls, nbp, codes, escm, hist, stage + loff);
+  else map32_stage<false>(in, ls, nbp, codes, escm, hist, stage + loff);
   {
     // zero bytes: all bytes that are not codes, escapes or padding
     const uint32_t nesc = __popc(escm);
@@ -229,6 +235,47 @@ struct Unmap32Smem {
   alignas(16) uint8_t stage[kUnmap32Warps][kGroupRecMax + 48];
 };
 
+// One lane's record (nw 8-byte words at rw) back to its values; returns the
+// bytes consumed. kFull: all 16 elements are valid (no per-element branch on
+// the count).
+template <bool kFull>
+__device__ __forceinline__ uint32_t unmap32_lane(const uint64_t* rw, uint32_t nw, uint32_t c,
+                                                 int cnt, uint32_t (&vals)[16], bool& bad) {
+  uint64_t A = nw > 0 ? rw[0] : 0ull, B = nw > 1 ? rw[1] : 0ull;
+  uint32_t blk = 0, cur = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    vals[i] = 0;
+    if (kFull || i < cnt) {
+      const uint32_t sh = 8u * (cur & 7u);
+      const uint64_t win = sh ? (A >> sh) | (B << (64u - sh)) : A;
+      const uint32_t lo = (uint32_t)win, hi = (uint32_t)(win >> 32);
+      uint32_t used;
+      if ((lo & 0xffu) == 254u) {
+        vals[i] = __byte_perm(lo, hi, 0x1234);  // big-endian literal, bytes 1..4
+        used = 5;
+      } else {
+        // leading zero bytes (at most 7), then the code byte
+        // (a window of eight zero bytes only occurs in a corrupt record)
+        const uint32_t z = min(7u, lo ? (uint32_t)(__ffs(lo) - 1) >> 3
+                                      : 4u + ((uint32_t)(__ffs(hi) - 1) >> 3));
+        const uint32_t code = (uint32_t)(win >> (8u * z)) & 0xffu;
+        bad |= (win == 0) | (code >= 254u);
+        const uint32_t d = (code >> 1) + 126u * z;
+        vals[i] = (code & 1u) ? c - d : c + d;
+        used = z + 1;
+      }
+      cur += used;
+      if ((cur >> 3) != blk) {  // crossed into the next word
+        ++blk;
+        A = B;
+        B = blk + 1 < nw ? rw[blk + 1] : 0ull;
+      }
+    }
+  }
+  return cur;
+}
+
 // Restore group `grp` of one buffer (one warp). rec_bytes: record bytes of
 // the merged buffer (validated by the caller); stage: the warp's
 // kGroupRecMax + 48 byte stage.
@@ -267,41 +314,11 @@ __device__ __forceinline__ void unmap32_group(const uint8_t* __restrict__ M, uin
   // read as zeros, so a corrupt record never reads outside it.
   const uint64_t* rw = reinterpret_cast<const uint64_t*>(stage + phase16(src) + loff);
   const uint32_t nw = len >> 3;
-  uint64_t A = nw > 0 ? rw[0] : 0ull, B = nw > 1 ? rw[1] : 0ull;
-  uint32_t blk = 0;
   uint32_t vals[16];
-  uint32_t cur = 0;
   bool bad = false;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    vals[i] = 0;
-    if (i < cnt) {
-      const uint32_t sh = 8u * (cur & 7u);
-      const uint64_t win = sh ? (A >> sh) | (B << (64u - sh)) : A;
-      const uint32_t lo = (uint32_t)win, hi = (uint32_t)(win >> 32);
-      uint32_t used;
-      if ((lo & 0xffu) == 254u) {
-        vals[i] = __byte_perm(lo, hi, 0x1234);  // big-endian literal, bytes 1..4
-        used = 5;
-      } else {
-        // leading zero bytes (at most 7), then the code byte
-        // (a window of eight zero bytes only occurs in a corrupt record)
-        const uint32_t z = min(7u, lo ? (uint32_t)(__ffs(lo) - 1) >> 3
-                                      : 4u + ((uint32_t)(__ffs(hi) - 1) >> 3));
-        const uint32_t code = (uint32_t)(win >> (8u * z)) & 0xffu;
-        bad |= (win == 0) | (code >= 254u);
-        const uint32_t d = (code >> 1) + 126u * z;
-        vals[i] = (code & 1u) ? c - d : c + d;
-        used = z + 1;
-      }
-      cur += used;
-      if ((cur >> 3) != blk) {  // crossed into the next word
-        ++blk;
-        A = B;
-        B = blk + 1 < nw ? rw[blk + 1] : 0ull;
-      }
-    }
-  }
+  uint32_t cur;
+  if (cnt == 16) cur = unmap32_lane<true>(rw, nw, c, 16, vals, bad);
+  else cur = unmap32_lane<false>(rw, nw, c, cnt, vals, bad);
   bad |= cur > len;
   if (__any_sync(0xffffffffu, bad) && lane == 0) report(sink, MANS_ERR_CORRUPT, grp);
   if (cnt == 16) {
