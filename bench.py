@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="override the element count (profiling runs)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="mixed_c3: skip the end-to-end pass through host buffers")
     ap.add_argument("--no-sub", action="store_true",
                     help="default workload: skip the mixed_c3 / serve_c5 / reference_gpu sub-records")
     ap.add_argument("--sub-steps", type=int, default=3, help="mixed_c3 sub-record: timed steps")

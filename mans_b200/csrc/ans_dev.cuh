@@ -323,11 +323,11 @@ __device__ __forceinline__ bool build_decode_tables(const uint8_t* __restrict__ 
 }
 
 // ---- decode ----
-// Words staged in shared memory per warp (4 KiB): every block whose padded
-// word count fits -- all blocks of data that compresses at all -- decodes
-// from shared memory; a block with more words (a block of nearly
-// incompressible bytes) reads its words from global memory instead.
-constexpr uint32_t kDecStageWords = 2048;
+// Words staged in shared memory per warp (5 KiB): every block whose padded
+// word count fits -- all blocks but those of bytes that the coding expands by
+// a quarter or more -- decodes from shared memory; a block with more words
+// reads its words from global memory instead.
+constexpr uint32_t kDecStageWords = 2560;
 // Decoded bytes leave through a per-warp 512-byte stage, 16 steps at a time,
 // as one 16-byte store per lane.
 constexpr int kDecChunkSteps = 16;
