@@ -263,3 +263,23 @@ def test_div126_magic():
     """floor(a/126) == (a * 512 * 66577) >> 32 for every a the mappers use."""
     a = np.arange(0, 65661 + 1009, dtype=np.uint64)
     np.testing.assert_array_equal((a * 512 * 66577) >> 32, a // 126)
+
+
+@pytest.mark.parametrize("layout", [0, 1, 2])
+@pytest.mark.parametrize("n", [0, 1, 511, 512, 513, 4097, 70_001, 1 << 18])
+def test_parallel_oracle_equals_serial_u16(n, layout, oracle):
+    """The group- and block-parallel oracle (the judge of the full-size GPU
+    streams) gives exactly the serial oracle's bytes, which the golden
+    vectors pin to the reference."""
+    from mans_b200 import workloads as W
+    rng = np.random.default_rng(n + layout)
+    for x in (W.volume_u16(n, 4), rng.integers(0, 65536, n, dtype=np.uint16)):
+        np.testing.assert_array_equal(oracle.compress_par(x, 10, layout, threads=4),
+                                      oracle.compress(x, 10, layout))
+
+
+@pytest.mark.parametrize("n", [0, 1, 511, 513, 70_001, 1 << 18])
+def test_parallel_oracle_equals_serial_u32(n, oracle):
+    from mans_b200 import workloads as W
+    for x in (W.detector_u32(n, 2), W.quant_u32(n, 3)):
+        np.testing.assert_array_equal(oracle.compress_par(x, 11, threads=4), oracle.compress(x, 11))
