@@ -385,7 +385,7 @@ struct BatchEncSmem {
   uint64_t bar[kBWarps];
 };
 
-__global__ __launch_bounds__(kBThreads) void batch_encode_kernel(const BatchItem* __restrict__ items,
+__global__ __launch_bounds__(kBThreads, 4) void batch_encode_kernel(const BatchItem* __restrict__ items,
                                                                  BatchState* states, uint32_t count,
                                                                  Ctrl* ctrl,
                                                                  unsigned long long* flags,
@@ -401,8 +401,22 @@ __global__ __launch_bounds__(kBThreads) void batch_encode_kernel(const BatchItem
   __syncthreads();
   const uint32_t epoch = *((volatile uint32_t*)&ctrl->epoch);
   const uint64_t total = __ldcg(&ctrl->merged_size);
-  uint16_t* sout =
-      reinterpret_cast<uint16_t*>(slots + ((uint64_t)blockIdx.x * kBWarps + warp) * kEncSlotBytes);
+  // Two word slots per warp: a block's words wait in one for its stream
+  // offset while the warp encodes its next block into the other (the
+  // single-buffer encoder does the same; every claimed block publishes its
+  // aggregate before any wait, so the deferred look-backs complete).
+  uint16_t* const slot0 = reinterpret_cast<uint16_t*>(
+      slots + ((uint64_t)blockIdx.x * kBWarps + warp) * 2 * kEncSlotBytes);
+  uint32_t cur = 0;
+  EncPending pend{0xffffffffu, 0, 0, nullptr};
+  uint32_t pend_item = 0;
+  auto finish = [&](const EncPending& pb, uint32_t i) {
+    const BatchItem& bi = items[i];
+    BatchState* si = &states[i];
+    encode_finish<true>(bi.out, bi.out_cap, si->msize, bi.out_size, nullptr, si->pdf,
+                        flags + si->unit_base, epoch, (int)bi.prob_bits, item_sink(ctrl, si), pb,
+                        lane);
+  };
   uint32_t it = 0, pit = 0, cur_item = 0xffffffffu;
   auto base = [&](uint32_t i) { return (uint64_t)states[i].unit_base; };
   // the block prefetch_grids grids of warps ahead is prefetched into L2 (a
@@ -433,10 +447,20 @@ __global__ __launch_bounds__(kBThreads) void batch_encode_kernel(const BatchItem
     }
     const uint32_t blk = u - st->unit_base;
     const uint8_t* src = b.dtype == MANS_U8 ? b.in : b.m;
-    encode_block<true>(src, st->msize, b.out, b.out_cap, b.out_size, nullptr, st->pdf,
-                       flags + st->unit_base, epoch, (int)b.prob_bits, item_sink(ctrl, st),
-                       sm.table[warp], sm.in[warp], bar, parity, sout, blk, lane);
+    uint16_t* const sout = slot0 + cur * (kEncSlotBytes / 2);
+    uint32_t x;
+    const uint32_t nw = encode_words<false>(src, st->msize, blk, sm.table[warp], sm.in[warp], bar,
+                                            parity, sout, (int)b.prob_bits, item_sink(ctrl, st),
+                                            lane, x);
+    if (lane == 0)
+      st_flag(&flags[st->unit_base + blk],
+              make_flag(blk == 0 ? kFlagIncl : kFlagAgg, epoch, (nw + 7) & ~7u));
+    if (pend.b != 0xffffffffu) finish(pend, pend_item);
+    pend = EncPending{blk, nw, x, sout};
+    pend_item = it;
+    cur ^= 1u;
   }
+  if (pend.b != 0xffffffffu) finish(pend, pend_item);
   __syncthreads();
   if (t == 0) {
     __threadfence();
@@ -533,21 +557,43 @@ __global__ __launch_bounds__(kBThreads) void batch_decode_kernel(const BatchItem
   extern __shared__ __align__(16) uint8_t smem_raw[];
   BatchDecSmem& sm = *reinterpret_cast<BatchDecSmem*>(smem_raw);
   __shared__ uint32_t s_scan[kBWarps];
-  __shared__ uint32_t s_chunk;
+  __shared__ uint32_t s_claim[2];
   __shared__ int s_last, s_tables;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   uint64_t* bar = &sm.bar[warp];
   if (lane == 0) mbar_init(bar);
   uint32_t parity = 0;
   const uint64_t total = __ldcg(&ctrl->merged_size);
-  uint32_t it = 0, cur_item = 0xffffffffu;
+  uint32_t it = 0, pit = 0, cur_item = 0xffffffffu;
   auto base = [&](uint32_t i) { return (uint64_t)states[i].unit_base; };
-  while (true) {
-    __syncthreads();
-    if (t == 0) s_chunk = atomicAdd(&ctrl->tile_counter[1], 1u);
-    __syncthreads();
-    const uint32_t c = s_chunk;
-    if (c >= total) break;
+  // Chunks are claimed two ahead: while chunk c is decoded, thread 0 claims
+  // the chunk after next (its atomic's latency is hidden) and every warp
+  // prefetches into L2 the words of its block of the next chunk.
+  // Every barrier in the loop below is reached by all threads: c and nxt are
+  // read from shared memory between two barriers, so they are the same in
+  // every thread, and thread 0 writes a claim only after all have read.
+  if (t == 0) {
+    s_claim[0] = atomicAdd(&ctrl->tile_counter[1], 1u);
+    s_claim[1] = atomicAdd(&ctrl->tile_counter[1], 1u);
+  }
+  __syncthreads();
+  uint32_t c = s_claim[0], nxt = s_claim[1];
+  __syncthreads();  // all have read both claims before thread 0 writes the next
+  while (c < total) {
+    if (t == 0) s_claim[0] = atomicAdd(&ctrl->tile_counter[1], 1u);  // read after the barrier below
+    if (nxt < total && lane == 0) {
+      pit = find_item(pit, count, nxt, base);
+      const BatchState* ps = &states[pit];
+      const uint32_t pblk = (nxt - ps->unit_base) * kChunkBlocks + warp;
+      if (pblk < ps->nb) {
+        const uint8_t* pin = items[pit].in;
+        const uint2 bw = __ldg(reinterpret_cast<const uint2*>(pin + kAnsHeaderBytes + 2 * kAnsSyms +
+                                                               128ull * ps->nb) + pblk);
+        const uint32_t wn = ((bw.x & 0xffffu) + 7) & ~7u;
+        if ((uint64_t)bw.y + wn <= ps->cw)
+          prefetch_l2(pin + ans_overhead(ps->nb) + 2ull * bw.y, 2 * wn);
+      }
+    }
     it = find_item(it, count, c, base);  // uniform across the CTA
     const BatchItem& b = items[it];
     BatchState* st = &states[it];
@@ -559,13 +605,18 @@ __global__ __launch_bounds__(kBThreads) void batch_decode_kernel(const BatchItem
       if (!s_tables && t == 0) report(item_sink(ctrl, st), MANS_ERR_BAD_STREAM, it);
       cur_item = it;
     }
-    if (!s_tables) continue;
-    const uint32_t blk = (c - st->unit_base) * kChunkBlocks + warp;
-    if (blk < st->nb) {
-      uint8_t* dst = b.dtype == MANS_U8 ? b.out : b.m;
-      decode_block(b.in, st->nb, st->n_hdr, st->cw, (int)p, dst, sm.lut, &sm.warp[warp], bar,
-                   parity, item_sink(ctrl, st), blk, lane);
+    if (s_tables) {
+      const uint32_t blk = (c - st->unit_base) * kChunkBlocks + warp;
+      if (blk < st->nb) {
+        uint8_t* dst = b.dtype == MANS_U8 ? b.out : b.m;
+        decode_block(b.in, st->nb, st->n_hdr, st->cw, (int)p, dst, sm.lut, &sm.warp[warp], bar,
+                     parity, item_sink(ctrl, st), blk, lane);
+      }
     }
+    __syncthreads();  // the chunk is done (the table may be rebuilt); s_claim[0] is set
+    c = nxt;
+    nxt = s_claim[0];
+    __syncthreads();  // everyone has read s_claim[0] before thread 0 overwrites it
   }
   __syncthreads();
   if (t == 0) {
@@ -701,7 +752,7 @@ void init_batch_cfg(BatchCfg& c, const LaunchCfg& base) {
 }
 
 uint64_t batch_slot_bytes(const BatchCfg& c) {
-  return (uint64_t)c.sms * c.occ[kStageEncode] * kBWarps * kEncSlotBytes;
+  return (uint64_t)c.sms * c.occ[kStageEncode] * kBWarps * 2 * kEncSlotBytes;  // two per warp
 }
 
 // Map stage of dtype kind k: grid for the schedule's warps per CTA (the
