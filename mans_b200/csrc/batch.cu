@@ -168,7 +168,7 @@ __device__ __forceinline__ void unit_span(const BatchItem& b, uint64_t u, const 
 }
 
 template <uint32_t kDtype>
-__global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_map_kernel(const BatchItem* __restrict__ items,
+__global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : kDtype == MANS_U16 ? 4 : 5) void batch_map_kernel(const BatchItem* __restrict__ items,
                                                               BatchState* states, uint32_t count,
                                                               uint64_t total_units, Ctrl* ctrl,
                                                               unsigned long long* flags,
@@ -202,6 +202,35 @@ __global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_m
     }
     return k;
   };
+  // uint16: a unit waits in registers (its groups' front halves) for its
+  // offset while the warp maps the front of its next unit, whose length is
+  // published first; its look-back then finds its predecessors' lengths
+  // published instead of stalling on a predecessor that started at the same
+  // time. A pending unit is finished before the warp moves to another buffer,
+  // so that its histogram counts stay with its own buffer.
+  Map16Lane P[kU16MapUnit];
+  uint32_t p_grp = 0xffffffffu, p_len = 0, p_it = 0;
+  auto finish16 = [&]() {
+    const BatchItem& pb = items[p_it];
+    BatchState* pst = &states[p_it];
+    const Sink psink = item_sink(ctrl, pst);
+    const uint16_t* in16 = reinterpret_cast<const uint16_t*>(pb.in);
+    const uint64_t g = div_up_u64(pb.n, kAdmGroup);
+    unsigned long long* fl = flags + pb.flag_base;
+    uint32_t off = 0;
+    if (p_grp > 0) {
+      off = lookback_exclusive(fl, p_grp, epoch, psink);
+      if (lane == 0) st_flag(&fl[p_grp], make_flag(kFlagIncl, epoch, off + p_len));
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < kU16MapUnit; ++q) {
+      if ((uint64_t)p_grp * kU16MapUnit + q < g)
+        map16_back(in16, pb.n, pb.m, pb.m_cap, &pst->msize, p_grp * kU16MapUnit + q, off, P[q],
+                   psink, wh, lane);
+      off += P[q].L;
+    }
+    p_grp = 0xffffffffu;
+  };
   while (true) {
     const uint32_t u = warp_claim(&ctrl->tile_counter[kSlot], lane);
     if (u >= total_units) break;
@@ -215,6 +244,9 @@ __global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_m
     }
     it = owner(it, u);
     if (it != cur_item) {
+      if constexpr (kDtype == MANS_U16) {
+        if (p_grp != 0xffffffffu) finish16();
+      }
       if (cur_item != 0xffffffffu)
         hist_leave(mh, hslot, wh, item_hist(hists, hist_items, cur_item), lane);
       cur_item = it;
@@ -240,18 +272,12 @@ __global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_m
         }
       }
       if (lane == 0) st_flag(&fl[grp], make_flag(grp == 0 ? kFlagIncl : kFlagAgg, epoch, len));
-      uint32_t off = 0;
-      if (grp > 0) {
-        off = lookback_exclusive(fl, grp, epoch, sink);
-        if (lane == 0) st_flag(&fl[grp], make_flag(kFlagIncl, epoch, off + len));
-      }
+      if (p_grp != 0xffffffffu) finish16();
 #pragma unroll
-      for (uint32_t q = 0; q < kU16MapUnit; ++q) {
-        if ((uint64_t)grp * kU16MapUnit + q < g)
-          map16_back(in16, b.n, b.m, b.m_cap, &st->msize, grp * kU16MapUnit + q, off, S[q], sink,
-                     wh, lane);
-        off += S[q].L;
-      }
+      for (uint32_t q = 0; q < kU16MapUnit; ++q) P[q] = S[q];
+      p_grp = grp;
+      p_len = len;
+      p_it = it;
     } else if constexpr (kDtype == MANS_U32) {
       BatchMapSmem& sm = *reinterpret_cast<BatchMapSmem*>(smem_raw);
       map32_group(reinterpret_cast<const uint32_t*>(b.in), b.n, b.m, b.m_cap, flags + b.flag_base,
@@ -280,6 +306,9 @@ __global__ __launch_bounds__(kBThreads, kDtype == MANS_U32 ? 3 : 5) void batch_m
         for (uint32_t i = lane; i < len; i += 32) atomicAdd(&h[p[i]], 1u);
       }
     }
+  }
+  if constexpr (kDtype == MANS_U16) {
+    if (p_grp != 0xffffffffu) finish16();
   }
   if (cur_item != 0xffffffffu)
     hist_leave(mh, hslot, wh, item_hist(hists, hist_items, cur_item), lane);
