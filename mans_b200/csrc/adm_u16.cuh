@@ -174,6 +174,46 @@ __device__ __forceinline__ void map16_front(const uint16_t* __restrict__ in, uin
   a.acc = acc;
 }
 
+// A long lane's bit bytes (64 stream bits or more), regenerated byte by byte
+// from its elements and counted in hist. Out of line: rare, and its code
+// would otherwise crowd the instruction cache of the map loop.
+static __device__ __noinline__ void map16_long_lane(const uint16_t* __restrict__ in, uint64_t n,
+                                             uint32_t grp, int lane, int cnt, uint32_t c,
+                                             uint32_t pos, uint32_t L, uint8_t* dst,
+                                             uint32_t* hist) {
+  uint32_t w[8];
+  load_lane_u16(in, n, grp, lane, w);
+  uint32_t cur = 0, bi = 0, bp = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    if (i < cnt) {
+      uint32_t k, code;
+      adm_elem_u16(elem16(w, i), c, k, code);
+      while ((bp >> 3) > bi) {
+        dst[bi++] = (uint8_t)cur;
+        atomicAdd(&hist[cur], 1u);
+        cur = 0;
+      }
+      cur |= 0x80u >> (bp & 7);
+      bp += k;
+    }
+  }
+  while ((pos >> 3) > bi) {
+    dst[bi++] = (uint8_t)cur;
+    atomicAdd(&hist[cur], 1u);
+    cur = 0;
+  }
+  if (bi < L) {
+    if (pos < 8 * L) cur |= 0xffu >> (pos & 7);
+    dst[bi++] = (uint8_t)cur;
+    atomicAdd(&hist[cur], 1u);
+  }
+  for (; bi < L; ++bi) {
+    dst[bi] = 0;
+    atomicAdd(&hist[0], 1u);
+  }
+}
+
 // Second half, once the group's bit offset gexcl (in units of 32 bytes) is
 // known: the merged size (last group), the group's length (or prefix) and
 // center fields with their histogram counts, and the lanes' bit bytes. A
@@ -235,38 +275,7 @@ __device__ __forceinline__ void map16_back(const uint16_t* __restrict__ in, uint
       for (uint32_t b = 0; b < L; ++b)
         dst[b] = (uint8_t)(b < 8 ? (uint32_t)(a.acc >> (56 - 8 * b)) & 0xffu : rest);
     } else {
-      // Long lane: regenerate the stream byte by byte.
-      uint32_t w[8];
-      load_lane_u16(in, n, grp, lane, w);
-      uint32_t cur = 0, bi = 0, bp = 0;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        if (i < a.cnt) {
-          uint32_t k, code;
-          adm_elem_u16(elem16(w, i), c, k, code);
-          while ((bp >> 3) > bi) {
-            dst[bi++] = (uint8_t)cur;
-            atomicAdd(&hist[cur], 1u);
-            cur = 0;
-          }
-          cur |= 0x80u >> (bp & 7);
-          bp += k;
-        }
-      }
-      while ((pos >> 3) > bi) {
-        dst[bi++] = (uint8_t)cur;
-        atomicAdd(&hist[cur], 1u);
-        cur = 0;
-      }
-      if (bi < L) {
-        if (pos < 8 * L) cur |= 0xffu >> (pos & 7);
-        dst[bi++] = (uint8_t)cur;
-        atomicAdd(&hist[cur], 1u);
-      }
-      for (; bi < L; ++bi) {
-        dst[bi] = 0;
-        atomicAdd(&hist[0], 1u);
-      }
+      map16_long_lane(in, n, grp, lane, a.cnt, c, pos, L, dst, hist);
     }
   }
 }
