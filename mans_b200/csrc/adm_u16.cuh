@@ -99,24 +99,39 @@ struct Map16Lane {
   int cnt;        // valid elements of the lane
 };
 
+// x << s with the PTX rule for s >= 64 (the result is 0).
+__device__ __forceinline__ uint64_t shl_b64(uint64_t x, uint32_t s) {
+  uint64_t r;
+  asm("shl.b64 %0, %1, %2;" : "=l"(r) : "l"(x), "r"(s));
+  return r;
+}
+
 // Codes and unary stream of a lane's elements (kFull: all 16 valid, no
 // per-element branch): code bytes packed into codes, each counted in hist;
-// the stream's first 64 bits in acc, its length in pos.
+// the stream's first 64 bits in acc (left-aligned; meaningful when the
+// stream is shorter than 64 bits), its length in pos. Each element appends
+// "1" and k - 1 zeros at the bottom of acc, which is aligned once at the end.
 template <bool kFull>
 __device__ __forceinline__ void map16_elems(const uint32_t (&w)[8], uint32_t c, int cnt,
                                             uint32_t* hist, uint32_t (&codes)[4], uint64_t& acc,
                                             uint32_t& pos) {
+  uint32_t cb[16];
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
+    cb[i] = 0;
     if (kFull || i < cnt) {
       uint32_t k, code;
       adm_elem_u16(elem16(w, i), c, k, code);
-      codes[i >> 2] |= code << ((i & 3) * 8);
+      cb[i] = code;
       atomicAdd(&hist[code], 1u);
-      if (pos < 64) acc |= 0x8000000000000000ull >> pos;
+      acc = shl_b64((acc << 1) | 1ull, k - 1);  // k - 1 >= 64 only in a long lane
       pos += k;
     }
+    if ((i & 3) == 3)  // four code bytes per word
+      codes[i >> 2] = __byte_perm(__byte_perm(cb[i - 3], cb[i - 2], 0x1140u),
+                                  __byte_perm(cb[i - 1], cb[i], 0x1140u), 0x5410u);
   }
+  acc = (pos - 1u) < 63u ? acc << (64u - pos) : 0ull;
 }
 
 // First half of mapping group `grp` (one warp): everything that does not
@@ -167,8 +182,12 @@ __device__ __forceinline__ void map16_front(const uint16_t* __restrict__ in, uin
   if (pos < 64) {
     if (v12_empty) acc = ~0ull;
     else if (pos < 8 * a.L) acc |= tail_fill_mask(pos);
-    const uint32_t nb8 = a.L < 8 ? a.L : 8u;
-    for (uint32_t b = 0; b < nb8; ++b) atomicAdd(&hist[(uint32_t)(acc >> (56 - 8 * b)) & 0xffu], 1u);
+    const uint32_t hi = (uint32_t)(acc >> 32), lo = (uint32_t)acc;
+#pragma unroll
+    for (uint32_t b = 0; b < 8; ++b) {
+      const uint32_t byte = (b < 4 ? hi >> (24 - 8 * b) : lo >> (56 - 8 * b)) & 0xffu;
+      if (b < a.L) atomicAdd(&hist[byte], 1u);
+    }
     if (a.L > 8) atomicAdd(&hist[v12_empty ? 0xffu : 0u], a.L - 8);
   }
   a.acc = acc;
@@ -239,41 +258,40 @@ __device__ __forceinline__ void map16_back(const uint16_t* __restrict__ in, uint
   }
 
   // lengths (i32 written as two u16: M is only 2-byte aligned here, or u16 L)
-  // and center
-  if (lane == 0) {
-    if constexpr (kLayout == kLayoutV12) {
-      reinterpret_cast<uint16_t*>(p_len + 2ull * grp)[0] = (uint16_t)L;
-      atomicAdd(&hist[L & 0xff], 1u);
-      atomicAdd(&hist[(L >> 8) & 0xff], 1u);
-    } else {
-      reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[0] = (uint16_t)(gexcl & 0xffffu);
-      reinterpret_cast<uint16_t*>(p_len + 4ull * grp)[1] = (uint16_t)(gexcl >> 16);
-      atomicAdd(&hist[gexcl & 0xff], 1u);
-      atomicAdd(&hist[(gexcl >> 8) & 0xff], 1u);
-      atomicAdd(&hist[(gexcl >> 16) & 0xff], 1u);
-      atomicAdd(&hist[gexcl >> 24], 1u);
-      if (kLayout == kLayoutCpuV2 && (uint64_t)grp + 1 == g) {
-        const uint32_t tot = gexcl + L;  // the CPU layout's extra final prefix word
-        reinterpret_cast<uint16_t*>(p_len + 4ull * g)[0] = (uint16_t)(tot & 0xffffu);
-        reinterpret_cast<uint16_t*>(p_len + 4ull * g)[1] = (uint16_t)(tot >> 16);
-        atomicAdd(&hist[tot & 0xff], 1u);
-        atomicAdd(&hist[(tot >> 8) & 0xff], 1u);
-        atomicAdd(&hist[(tot >> 16) & 0xff], 1u);
-        atomicAdd(&hist[tot >> 24], 1u);
-      }
+  // and center, one store and one histogram byte per lane
+  {
+    constexpr uint32_t nlen = kLayout == kLayoutV12 ? 2 : 4;  // length field bytes
+    const uint32_t lenv = kLayout == kLayoutV12 ? L : gexcl;
+    if ((uint32_t)lane < nlen) atomicAdd(&hist[(lenv >> (8 * lane)) & 0xffu], 1u);
+    else if ((uint32_t)lane < nlen + 2) atomicAdd(&hist[(c >> (8 * (lane - nlen))) & 0xffu], 1u);
+    if ((uint32_t)lane < nlen / 2)
+      reinterpret_cast<uint16_t*>(p_len + (uint64_t)nlen * grp)[lane] =
+          (uint16_t)(lenv >> (16 * lane));
+    else if ((uint32_t)lane == nlen / 2)
+      reinterpret_cast<uint16_t*>(p_ctr + 2ull * grp)[0] = (uint16_t)c;
+    if (kLayout == kLayoutCpuV2 && (uint64_t)grp + 1 == g && lane == 0) {
+      const uint32_t tot = gexcl + L;  // the CPU layout's extra final prefix word
+      reinterpret_cast<uint16_t*>(p_len + 4ull * g)[0] = (uint16_t)(tot & 0xffffu);
+      reinterpret_cast<uint16_t*>(p_len + 4ull * g)[1] = (uint16_t)(tot >> 16);
+      atomicAdd(&hist[tot & 0xff], 1u);
+      atomicAdd(&hist[(tot >> 8) & 0xff], 1u);
+      atomicAdd(&hist[(tot >> 16) & 0xff], 1u);
+      atomicAdd(&hist[tot >> 24], 1u);
     }
-    reinterpret_cast<uint16_t*>(p_ctr + 2ull * grp)[0] = (uint16_t)c;
-    atomicAdd(&hist[c & 0xff], 1u);
-    atomicAdd(&hist[(c >> 8) & 0xff], 1u);
   }
   // bits: lane region [32*gexcl + lane*L, +L) of the bits section
   const uint64_t gend = bits_base + 32ull * ((uint64_t)gexcl + L);
   if (gend <= m_cap) {
     uint8_t* dst = p_bits + 32ull * gexcl + (uint64_t)lane * L;
     if (pos < 64) {
-      const uint32_t rest = (kLayout == kLayoutV12 && a.cnt == 0) ? 0xffu : 0u;
-      for (uint32_t b = 0; b < L; ++b)
-        dst[b] = (uint8_t)(b < 8 ? (uint32_t)(a.acc >> (56 - 8 * b)) & 0xffu : rest);
+      const uint32_t hi = (uint32_t)(a.acc >> 32), lo = (uint32_t)a.acc;
+#pragma unroll
+      for (uint32_t b = 0; b < 8; ++b)
+        if (b < L) dst[b] = (uint8_t)(b < 4 ? hi >> (24 - 8 * b) : lo >> (56 - 8 * b));
+      if (L > 8) {
+        const uint8_t rest = (kLayout == kLayoutV12 && a.cnt == 0) ? 0xffu : 0u;
+        for (uint32_t b = 8; b < L; ++b) dst[b] = rest;
+      }
     } else {
       map16_long_lane(in, n, grp, lane, a.cnt, c, pos, L, dst, hist);
     }
@@ -393,7 +411,9 @@ __device__ __forceinline__ void unmap16_group(const uint8_t* __restrict__ M, uin
   bool bad = false;
   if (L <= 8) {
     uint64_t acc = 0;
-    for (uint32_t b = 0; b < L; ++b) acc |= (uint64_t)src[b] << (56 - 8 * b);
+#pragma unroll
+    for (uint32_t b = 0; b < 8; ++b)  // all loads in flight at once
+      if (b < L) acc |= (uint64_t)__ldg(src + b) << (56 - 8 * b);
     if (cnt == 16) bad = unary_signals<true>(acc, (int)L, 16, sig);
     else bad = unary_signals<false>(acc, (int)L, cnt, sig);
   } else {
