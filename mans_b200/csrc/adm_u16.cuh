@@ -51,12 +51,13 @@ __device__ __forceinline__ uint32_t div126(uint32_t a) {
   return __umulhi(a << 9, 66577u);
 }
 
-// k = max(1, ceil(d/126)), code = 2r + (v <= c), r = d + 126 - 126k.
+// k = max(1, ceil(d/126)), code = 2r + (v <= c), r = d + 126 - 126k, i.e.
+// code = 2d + 252 + (v <= c) - 252k; (d + 125) << 9 is one multiply-add.
 __device__ __forceinline__ void adm_elem_u16(uint32_t v, uint32_t c, uint32_t& k, uint32_t& code) {
-  const uint32_t d = (uint32_t)abs((int)v - (int)c);
-  k = max(1u, div126(d + 125u));
-  const uint32_t r = d + 126u - 126u * k;
-  code = 2u * r + (v <= c ? 1u : 0u);
+  const int s = (int)v - (int)c;
+  const uint32_t d = (uint32_t)abs(s);
+  k = max(1u, __umulhi(d * 512u + 64000u, 66577u));
+  code = d + d + (s <= 0 ? 253u : 252u) - 252u * k;
 }
 
 __device__ __forceinline__ uint32_t elem16(const uint32_t (&w)[8], int i) {
@@ -152,9 +153,15 @@ __device__ __forceinline__ void map16_front(const uint16_t* __restrict__ in, uin
   a.cnt = ls >= n ? 0 : (int)min_u64(16, n - ls);
 
   // ---- center: truncated mean (u32 sum of at most 512 uint16 values)
-  uint32_t lsum = 0;
+  // sum of the 16 halves: S = sum of the words (mod 2^32) counts each high
+  // half 65536 times, so the halves sum to S - 65535 * (sum of high halves)
+  uint32_t wsum = 0, hsum = 0;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) lsum += (w[i] & 0xffffu) + (w[i] >> 16);
+  for (int i = 0; i < 8; ++i) {
+    wsum += w[i];
+    hsum += w[i] >> 16;
+  }
+  const uint32_t lsum = wsum - 65535u * hsum;
   const uint32_t gsum = __reduce_add_sync(0xffffffffu, lsum);
   const uint32_t gcnt = (uint32_t)min_u64(kAdmGroup, n - gs);
   a.c = gcnt == kAdmGroup ? (gsum >> 9) : gsum / gcnt;
