@@ -339,29 +339,39 @@ __device__ __forceinline__ uint32_t rd_u32_2aligned(const uint8_t* p) {
   return (uint32_t)q[0] | ((uint32_t)q[1] << 16);
 }
 
-// The signal counts of a lane's unary stream held left-aligned in acc (L <= 8
-// bytes): per element, the zeros after its leading 1. Returns true when the
-// stream is malformed. kFull: all 16 elements are valid (no per-element
-// branch).
-template <bool kFull>
-__device__ __forceinline__ bool unary_signals(uint64_t acc, int L, int cnt, uint32_t (&sig)[16]) {
-  // win: the stream from the current element's leading 1, left-aligned;
-  // left: its bits that are still in the lane's record
-  uint64_t win = acc;
-  int left = 8 * L;
-  bool bad = false;
+__device__ __forceinline__ uint32_t shl_w(uint32_t x, uint32_t s) {  // 0 for s >= 32
+  uint32_t r;
+  asm("shl.b32 %0, %1, %2;" : "=r"(r) : "r"(x), "r"(s));
+  return r;
+}
+__device__ __forceinline__ uint64_t shl_w(uint64_t x, uint32_t s) { return shl_b64(x, s); }
+__device__ __forceinline__ int clz_w(uint32_t x) { return __clz(x); }
+__device__ __forceinline__ int clz_w(uint64_t x) { return __clzll(x); }
+
+// The signal counts of a lane's unary stream held left-aligned in acc (a
+// 32-bit word when the group's lanes take at most 4 bytes, else 64 bits;
+// nbits = 8L): per element, the zeros after its leading 1. Element i starts
+// at bit s (s = 0 for the first); its signal is the distance to the next 1
+// bit, at most to the lane's end, and the next element starts there. The
+// stream is malformed when it does not start with a 1 or an element starts
+// at or past the lane's end (s only grows, so the last element's start
+// decides). Returns true when malformed. kFull: all 16 elements are valid
+// (no per-element branch).
+template <bool kFull, typename W>
+__device__ __forceinline__ bool unary_signals(W acc, int nbits, int cnt, uint32_t (&sig)[16]) {
+  constexpr int kTop = 8 * (int)sizeof(W) - 1;
+  bool bad = (kFull || cnt > 0) && !(acc >> kTop);
+  int s = 0;
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     sig[i] = 0;
     if (kFull || i < cnt) {
-      bad |= left <= 0 || !(win >> 63);
-      const uint64_t rest = win << 1;
-      int z = rest ? __clzll(rest) : 64;
-      const int lim = left > 1 ? left - 1 : 0;
-      z = z < lim ? z : lim;
-      sig[i] = (uint32_t)z;
-      win = z < 63 ? rest << z : 0ull;  // advance by z + 1 bits
-      left -= z + 1;
+      if (!kFull || i == 15) bad |= s >= nbits;
+      const int t = s + 1;
+      const int z = clz_w(shl_w(acc, (uint32_t)t));
+      const int g = min(z, max(nbits - t, 0));
+      sig[i] = (uint32_t)g;
+      s = t + g;
     }
   }
   return bad;
@@ -421,8 +431,14 @@ __device__ __forceinline__ void unmap16_group(const uint8_t* __restrict__ M, uin
 #pragma unroll
     for (uint32_t b = 0; b < 8; ++b)  // all loads in flight at once
       if (b < L) acc |= (uint64_t)__ldg(src + b) << (56 - 8 * b);
-    if (cnt == 16) bad = unary_signals<true>(acc, (int)L, 16, sig);
-    else bad = unary_signals<false>(acc, (int)L, cnt, sig);
+    if (L <= 4) {
+      const uint32_t a32 = (uint32_t)(acc >> 32);
+      if (cnt == 16) bad = unary_signals<true>(a32, (int)(8 * L), 16, sig);
+      else bad = unary_signals<false>(a32, (int)(8 * L), cnt, sig);
+    } else {
+      if (cnt == 16) bad = unary_signals<true>(acc, (int)(8 * L), 16, sig);
+      else bad = unary_signals<false>(acc, (int)(8 * L), cnt, sig);
+    }
   } else {
     // Long lanes: scan byte by byte like the reference.
     int idx = -1;
@@ -450,11 +466,11 @@ __device__ __forceinline__ void unmap16_group(const uint8_t* __restrict__ M, uin
     uint32_t r[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const uint32_t code = (codes[(i + h) >> 2] >> (((i + h) & 3) * 8)) & 0xffu;
+      const uint32_t code = __byte_perm(codes[(i + h) >> 2], 0u, 0x4440u | ((i + h) & 3));
       const uint32_t d = (code >> 1) + 126u * sig[i + h];
-      r[h] = ((code & 1u) ? c - d : c + d) & 0xffffu;
+      r[h] = (code & 1u) ? c - d : c + d;
     }
-    vals[i >> 1] = r[0] | (r[1] << 16);
+    vals[i >> 1] = __byte_perm(r[0], r[1], 0x5410u);  // low halves of both
   }
   if (cnt == 16) {
     uint4* o = reinterpret_cast<uint4*>(out + ls);
