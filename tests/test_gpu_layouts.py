@@ -85,6 +85,43 @@ def test_layout_header_corruption_is_reported(ws, oracle):
     assert e.value.code == 10
 
 
+def test_u16_malformed_lane_streams_are_reported(ws, oracle):
+    """Lane bit streams that cannot be decoded are reported as corrupt (status
+    10): a lane whose stream does not start with a 1, and a lane whose
+    elements run past its bytes. The faults are planted in the oracle's
+    mapped buffer on the CPU, in a group whose lanes take at most 4 bytes
+    (decoded on 32-bit words) and in one whose lanes take 5 to 8 (64 bits);
+    the untouched buffers decode to the input."""
+    import torch
+    n = 512 * 16
+    g = n // 512
+    for gen, seed, lo, hi in ((W.laplace_u16, 11, 1, 4), (W.volume_u16, 12, 5, 8)):
+        x = gen(n, seed)
+        m0 = oracle.adm_u16_map(x)
+        pre = m0[:4 * g].copy().view(np.int32)  # exclusive prefix, 32-byte units
+        bits = 6 * g + n
+        tot = (m0.size - bits) // 32
+        lens = np.diff(np.append(pre, tot))
+        grps = np.nonzero((lens >= lo) & (lens <= hi))[0]
+        assert grps.size, (gen.__name__, lens)
+        grp = int(grps[0])
+        L = int(lens[grp])
+        base = bits + 32 * int(pre[grp])
+        back = mb.adm_unmap(to_dev(m0), n, torch.uint16, ws=ws)
+        np.testing.assert_array_equal(to_host(back, np.uint16), x)
+        m = m0.copy()
+        m[base + 5 * L] &= 0x7F  # lane 5 no longer starts with a 1
+        with pytest.raises(mb.MansError) as e:
+            mb.adm_unmap(to_dev(m), n, torch.uint16, ws=ws)
+        assert e.value.code == 10
+        m = m0.copy()
+        m[base + 7 * L] = 0x80  # lane 7: one leading 1, then zeros to its end
+        m[base + 7 * L + 1:base + 8 * L] = 0
+        with pytest.raises(mb.MansError) as e:
+            mb.adm_unmap(to_dev(m), n, torch.uint16, ws=ws)
+        assert e.value.code == 10
+
+
 def test_layout_argument_checks(ws):
     import torch
     x = torch.zeros(1024, dtype=torch.uint32, device="cuda")
