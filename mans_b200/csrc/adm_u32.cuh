@@ -248,7 +248,9 @@ __device__ __forceinline__ uint32_t unmap32_lane(const uint64_t* rw, uint32_t nw
     vals[i] = 0;
     if (kFull || i < cnt) {
       const uint32_t sh = 8u * (cur & 7u);
-      const uint64_t win = sh ? (A >> sh) | (B << (64u - sh)) : A;
+      uint64_t bsh;  // B << (64 - sh), 0 for sh == 0 (PTX clamps the shift)
+      asm("shl.b64 %0, %1, %2;" : "=l"(bsh) : "l"(B), "r"(64u - sh));
+      const uint64_t win = (A >> sh) | bsh;
       const uint32_t lo = (uint32_t)win, hi = (uint32_t)(win >> 32);
       uint32_t used;
       if ((lo & 0xffu) == 254u) {
@@ -259,7 +261,7 @@ __device__ __forceinline__ uint32_t unmap32_lane(const uint64_t* rw, uint32_t nw
         // (a window of eight zero bytes only occurs in a corrupt record)
         const uint32_t z = min(7u, lo ? (uint32_t)(__ffs(lo) - 1) >> 3
                                       : 4u + ((uint32_t)(__ffs(hi) - 1) >> 3));
-        const uint32_t code = (uint32_t)(win >> (8u * z)) & 0xffu;
+        const uint32_t code = __byte_perm(lo, hi, z) & 0xffu;  // byte z of the window
         bad |= (win == 0) | (code >= 254u);
         const uint32_t d = (code >> 1) + 126u * z;
         vals[i] = (code & 1u) ? c - d : c + d;
