@@ -262,7 +262,7 @@ __device__ __forceinline__ uint32_t unmap32_lane(const uint64_t* rw, uint32_t nw
         const uint32_t z = min(7u, lo ? (uint32_t)(__ffs(lo) - 1) >> 3
                                       : 4u + ((uint32_t)(__ffs(hi) - 1) >> 3));
         const uint32_t code = __byte_perm(lo, hi, z) & 0xffu;  // byte z of the window
-        bad |= (win == 0) | (code >= 254u);
+        bad |= code - 1u >= 253u;  // 0 (an all-zero window), 254 or 255
         const uint32_t d = (code >> 1) + 126u * z;
         vals[i] = (code & 1u) ? c - d : c + d;
         used = z + 1;
