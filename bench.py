@@ -506,8 +506,10 @@ def run_mans(args):
         if it > 0:
             e2e_seq_ms.append(a.elapsed_time(b))
     e2e_ok = bool(torch.equal(sets[0]["h_out"], h_in))
-    # (b): one untimed warm-up round, then the timed sequence
-    n_pipe = max(4, 2 * args.e2e_steps)
+    # (b): one untimed warm-up round, then the timed sequence; long enough
+    # that filling and draining the pipeline (one step's full chain of
+    # copies and kernels) is a small part of the time per step
+    n_pipe = max(16, 4 * args.e2e_steps)
     for timed in (False, True):
         if dist:
             dist.barrier()
