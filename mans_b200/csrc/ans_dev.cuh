@@ -28,9 +28,9 @@ struct alignas(16) EncEntry4 {
   uint32_t rcp, thr, bias, cs;
 };
 __device__ __forceinline__ EncEntry4 expand_enc_entry(uint2 e, int p) {
-  const uint32_t cmpl = (e.y >> 13) & 0xfffu;
-  return EncEntry4{e.x, ((1u << p) - cmpl) << (kAnsStateBits - p), e.y & 0x1fffu,
-                   (e.y >> 25) | (cmpl << 5)};
+  const uint32_t cmpl = e.y >> 20;
+  return EncEntry4{e.x, ((1u << p) - cmpl) << (kAnsStateBits - p), (e.y >> 5) & 0x1fffu,
+                   (e.y & 31u) | (cmpl << 5)};
 }
 
 struct EncSmemSlots {  // words go to global slots
@@ -55,9 +55,8 @@ struct EncSmem {  // words compacted in shared memory
 // x' = (xr / pdf << p) + xr % pdf + cdf = xr + bias + q * cmpl, q = xr / pdf.
 template <int kP>
 __device__ __forceinline__ uint32_t enc_code(uint32_t xr, const uint2& e) {
-  const uint32_t cmpl = (e.y >> 13) & 0xfffu;
-  const uint32_t q = __umulhi(xr, e.x) >> (e.y >> 25);
-  return xr + (e.y & 0x1fffu) + q * cmpl;
+  const uint32_t q = __funnelshift_r(__umulhi(xr, e.x), 0u, e.y);  // shift = y & 31
+  return xr + ((e.y >> 5) & 0x1fffu) + q * (e.y >> 20);
 }
 template <int kP>
 __device__ __forceinline__ uint32_t enc_code(uint32_t xr, const EncEntry4& e) {
@@ -66,7 +65,7 @@ __device__ __forceinline__ uint32_t enc_code(uint32_t xr, const EncEntry4& e) {
 }
 template <int kP>
 __device__ __forceinline__ uint32_t enc_threshold(const uint2& e) {
-  return ((1u << kP) - ((e.y >> 13) & 0xfffu)) << (kAnsStateBits - kP);
+  return ((1u << kP) - (e.y >> 20)) << (kAnsStateBits - kP);
 }
 template <int kP>
 __device__ __forceinline__ uint32_t enc_threshold(const EncEntry4& e) {

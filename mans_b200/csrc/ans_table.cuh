@@ -7,8 +7,10 @@ namespace mans {
 
 // Encoder table entry for one symbol:
 //   x = rcp   : ceil(2^(31+l) / pdf) with l = ceil(log2 pdf) (0xffffffff for pdf 1)
-//   y = bias | cmpl << 13 | shift << 25
+//   y = shift | bias << 5 | cmpl << 20
 //       bias  = cdf (cdf + 2^p - 1 for pdf 1), cmpl = 2^p - pdf, shift = l - 1
+//       (shift in the low five bits: a wrapping funnel shift applies it as
+//       it stands)
 // so that for a state x < 2^31:
 //   q  = umulhi(x, rcp) >> shift          == x / pdf        (exact, below)
 //   x' = x + bias + q * cmpl              == (x/pdf << p) + x%pdf + cdf
@@ -23,12 +25,12 @@ __host__ __device__ inline uint2 make_enc_entry(uint32_t pdf, uint32_t cdf, int 
   if (pdf <= 1) {
     // pdf == 0 (absent symbol) is never encoded; keep a harmless entry.
     uint32_t bias = cdf + (1u << p) - 1;
-    return make_uint2(0xffffffffu, bias | ((cmpl & 0xfffu) << 13) | (0u << 25));
+    return make_uint2(0xffffffffu, 0u | (bias << 5) | ((cmpl & 0xfffu) << 20));
   }
   uint32_t l = 0;
   while ((1u << l) < pdf) ++l;
   uint64_t rcp = ((1ull << (31 + l)) + pdf - 1) / pdf;
-  return make_uint2((uint32_t)rcp, cdf | (cmpl << 13) | ((l - 1) << 25));
+  return make_uint2((uint32_t)rcp, (l - 1) | (cdf << 5) | (cmpl << 20));
 }
 
 // Probability normalisation of one histogram, executed by one CTA of exactly

@@ -49,7 +49,7 @@ struct Ctrl {
   uint32_t tile_counter[8];   // dynamic work counters, reset by the last CTA
   uint32_t done_counter[8];   // CTA completion counters, reset by the last CTA
   uint32_t hist[kAnsSyms];    // histogram of the merged bytes
-  uint2 enc_table[kAnsSyms];  // {reciprocal, bias | cmpl << 12 | shift << 24}
+  uint2 enc_table[kAnsSyms];  // {reciprocal, shift | bias << 5 | cmpl << 20}
   uint32_t pdf[kAnsSyms];
   unsigned long long merged_size;  // merged bytes of the current call
   uint32_t total_words;

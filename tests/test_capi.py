@@ -97,7 +97,7 @@ def test_division_table_is_exact():
             cdf = int(rng.integers(0, M - pdf + 1))
             lib.mans_debug_enc_entry(pdf, cdf, p, out)
             rcp, y = int(out[0]), int(out[1])
-            bias, cmpl, sh = y & 0x1FFF, (y >> 13) & 0xFFF, y >> 25
+            sh, bias, cmpl = y & 0x1F, (y >> 5) & 0x1FFF, y >> 20
             assert cmpl == M - pdf
             hi = pdf << (31 - p)
             x = np.concatenate([rng.integers(1, hi, 2000, dtype=np.uint64),
