@@ -177,6 +177,34 @@ def test_oracle_u16_extreme_values(oracle):
     np.testing.assert_array_equal(oracle.adm_u16_unmap(m, x.size), x)
 
 
+def test_oracle_u16_rejects_malformed_lane_streams(oracle):
+    """The reference's restore (mappingcpuV2.cpp:161-197, restated by the
+    oracle) rejects a lane stream that does not start with a 1 and one that
+    holds fewer elements than the lane: the two faults the GPU unmap must
+    report as corrupt (tests/test_gpu_layouts.py plants the same ones)."""
+    n = 512 * 16
+    g = n // 512
+    for gen, seed in ((W.laplace_u16, 11), (W.volume_u16, 12)):
+        x = gen(n, seed)
+        m0 = oracle.adm_u16_map(x)
+        pre = m0[:4 * g].copy().view(np.int32)
+        bits = 6 * g + n
+        lens = np.diff(np.append(pre, (m0.size - bits) // 32))
+        for grp in (0, int(np.argmax(lens))):
+            L = int(lens[grp])
+            base = bits + 32 * int(pre[grp])
+            m = m0.copy()
+            m[base + 5 * L] &= 0x7F  # lane 5: no leading 1
+            with pytest.raises(ValueError, match="-4"):
+                oracle.adm_u16_unmap(m, n)
+            m = m0.copy()
+            m[base + 7 * L] = 0x80  # lane 7: one element, then zeros to its end
+            m[base + 7 * L + 1:base + 8 * L] = 0
+            with pytest.raises(ValueError, match="-5"):
+                oracle.adm_u16_unmap(m, n)
+        np.testing.assert_array_equal(oracle.adm_u16_unmap(m0, n), x)
+
+
 @pytest.mark.parametrize("n", [0, 1, 16, 513, 4096, 70001])
 def test_oracle_u32_roundtrip(n, oracle):
     for x in (W.detector_u32(n, 12), W.quant_u32(n, 13),
