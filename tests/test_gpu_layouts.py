@@ -122,6 +122,40 @@ def test_u16_malformed_lane_streams_are_reported(ws, oracle):
         assert e.value.code == 10
 
 
+def _u32_lane_record(m, n, grp, lane):
+    """Offset and length of one lane's record in a uint32 mapped buffer:
+    [i32 group offset x g][u32 center x g][u8 length / 8 x 32 g][records]."""
+    g = -(-n // 512)
+    goff = int(m[4 * grp:4 * grp + 4].view(np.uint32)[0])
+    lens = 8 * m[8 * g + 32 * grp:8 * g + 32 * grp + 32].astype(np.int64)
+    return 40 * g + goff + int(lens[:lane].sum()), int(lens[lane])
+
+
+def test_u32_malformed_records_are_reported(ws, oracle):
+    """uint32 records that cannot be parsed are reported as corrupt (status
+    10): a lane record of zero bytes only, and a padding byte (255) where a
+    code byte belongs. Planted in the oracle's mapped buffer on the CPU; the
+    oracle rejects both too."""
+    import torch
+    n = 512 * 8
+    x = W.quant_u32(n, 21)
+    m0 = oracle.adm_u32_map(x)
+    np.testing.assert_array_equal(to_host(mb.adm_unmap(to_dev(m0), n, torch.uint32, ws=ws),
+                                          np.uint32), x)
+    start, ln = _u32_lane_record(m0, n, 3, 9)
+    m = m0.copy()
+    m[start:start + ln] = 0
+    m2 = m0.copy()
+    first = start + int(np.nonzero(m0[start:start + ln])[0][0])  # the lane's first nonzero byte
+    m2[first] = 255
+    for bad in (m, m2):
+        with pytest.raises(ValueError):
+            oracle.adm_u32_unmap(bad, n)
+        with pytest.raises(mb.MansError) as e:
+            mb.adm_unmap(to_dev(bad), n, torch.uint32, ws=ws)
+        assert e.value.code == 10
+
+
 def test_layout_argument_checks(ws):
     import torch
     x = torch.zeros(1024, dtype=torch.uint32, device="cuda")
