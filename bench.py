@@ -227,7 +227,7 @@ def cpu_round_trip(workload: str, n: int, reps: int, warm: int, seed: int = 7) -
     x = gen_host_sample(workload, n, seed)
     r = cpu_round_trip_array(x, reps, warm, f"the same generator, seed {seed}")
     x1 = x[: max(1, (x.size // 16) // 512 * 512)]
-    r1 = cpu_round_trip_array(x1, 1, 1, f"the same generator, seed {seed}", threads=1)
+    r1 = cpu_round_trip_array(x1, 3, 1, f"the same generator, seed {seed}", threads=1)
     r["one_thread"] = {"value": r1["value"], "unit": r1["unit"], "sample": r1["sample"]}
     return r
 
