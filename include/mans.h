@@ -402,7 +402,9 @@ const char* mans_version(void);
 mans_status mans_debug_bounded_wait(uint32_t* status, float* elapsed_ms);
 
 /* Diagnostic: the encoder's division-table entry {reciprocal, packed} for a
- * symbol of probability pdf / 2^p and cumulative frequency cdf. */
+ * symbol of probability pdf / 2^p and cumulative frequency cdf; packed =
+ * shift | bias << 5 | (2^p - pdf) << 20, with x / pdf = umulhi(x, rcp) >>
+ * shift for every state the encoder holds. */
 void mans_debug_enc_entry(uint32_t pdf, uint32_t cdf, int p, uint32_t out[2]);
 
 #ifdef __cplusplus
